@@ -1,0 +1,279 @@
+"""Seeded synthetic workloads for the shot solver.
+
+No public dataset exists for these cases, so every model, geometry and
+wavelet is generated here from ``numpy.random.default_rng(seed)``:
+
+* ``plain_elastic`` -- 400 x 160 grid, DH 1 m, FDORDER 4 Taylor, CPML 20 cells
+  on the sides and bottom, free surface, linear vp 1800->2800 m/s, vs=vp/1.73,
+  Gardner-type rho = 310 vp^0.25, a +10 % circular vp/vs anomaly (radius 15
+  cells) in the true model, Ricker 40 Hz, dt = 0.9 x the CFL limit, NT 2000,
+  8 explosive shots and 100 receivers at 3 cells depth, DTINV 2;
+* ``visco_layered`` -- 2000 x 600 grid, DH 2 m, FDORDER 8 Holberg (0.1 %),
+  L=3 relaxation mechanisms fit to Q=20 over 5-60 Hz, 12 seeded layers
+  vp 1500-4500 m/s plus 3 seeded dipping faults, 64 shots, 400 receivers,
+  Ricker 15 Hz, NT 6000, DTINV 3;
+* ``batched_perturbed`` -- 256 shots over the plain_elastic start model and
+  4 seeded perturbations of it;
+* ``precision_layered`` -- 4000 x 1200 grid, DH 2.5 m, FDORDER 8, layered and
+  faulted vp 1500-5500 m/s times (1 + 0.15 G) with G a unit-variance Gaussian
+  random field of 50 m correlation length, 128 shots, NT 8000;
+* ``serving_stream`` -- a seeded Poisson stream of mixed requests.
+
+Models are float32 planes NY x NX, row-major with x fastest, j=1 (the free
+surface) first.  ``write_model`` writes them in the reference's file order
+(x outer, y inner; src/readmod_elastic.c).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .params import ShotParams, iround
+
+# Sum of |hc| per FDORDER and MAXRELERROR, for the CFL limit
+# DT <= DH / (sqrt(2) * sum|hc| * vmax)  (src/checkfd_ssg_elastic.c:105-106).
+_TAYLOR = {2: [1.0], 4: [9 / 8, -1 / 24], 6: [75 / 64, -25 / 384, 3 / 640],
+           8: [1225 / 1024, -245 / 3072, 49 / 5120, -5 / 7168]}
+_HOLBERG_01 = {8: [1.2257, -0.099537, 0.018063, -0.0026274], 4: [1.1382, -0.046414],
+               12: [1.2508, -0.12034, 0.032131, -0.010142, 0.0029857, -0.00066667]}
+
+
+def cfl_dt(dh: float, vmax: float, coeff_sum: float, frac: float = 0.9) -> float:
+    return float(np.float32(frac * dh / (math.sqrt(2.0) * coeff_sum * vmax)))
+
+
+def gardner_rho(vp):
+    return (310.0 * np.power(vp, 0.25)).astype(np.float32)
+
+
+@dataclass
+class Geometry:
+    """Sources in the reference's srcpos_loc row layout (8 x nsrc) and
+    receivers as 1-based grid indices (2 x ntr)."""
+    srcpos: np.ndarray
+    recpos: np.ndarray
+
+
+def source_rows(p: ShotParams, xs_m, ys_m, fc, amp=1.0, tshift=0.0, azimuth=0.0, stype=None) -> np.ndarray:
+    """Grid-located sources as ``splitsrc`` produces them for one rank
+    (src/splitsrc.c:35-50): index = iround(x/DH) in float arithmetic."""
+    xs_m = np.atleast_1d(np.asarray(xs_m, np.float32))
+    ys_m = np.atleast_1d(np.asarray(ys_m, np.float32))
+    n = xs_m.size
+    rows = np.zeros((8, n), np.float32)
+    dh = np.float32(p.dh)
+    for l in range(n):
+        ix = iround(float(np.float32(xs_m[l] / dh)))
+        iy = iround(float(np.float32(ys_m[l] / dh)))
+        rows[0, l] = ((ix - 1) % p.nx) + 1 if ix >= 1 else ix
+        rows[1, l] = ((iy - 1) % p.ny) + 1 if iy >= 1 else iy
+        rows[3, l] = tshift
+        rows[4, l] = fc
+        rows[5, l] = amp
+        rows[6, l] = azimuth
+        rows[7, l] = p.source_type if stype is None else stype
+    return rows
+
+
+def receiver_rows(p: ShotParams, xr_m, yr_m) -> np.ndarray:
+    """Receiver grid indices as ``receiver`` computes them from a file
+    (src/receiver.c:58-60, float parse then iround((x+REFREC)/DH)) with
+    same-cell duplicates removed in file order (src/receiver.c:73-88)."""
+    dh = np.float32(p.dh)
+    out = []
+    seen = set()
+    for x, y in zip(np.asarray(xr_m, np.float32), np.asarray(yr_m, np.float32)):
+        ix = iround(float(np.float32((x + np.float32(p.refrecx)) / dh)))
+        iy = iround(float(np.float32((y + np.float32(p.refrecy)) / dh)))
+        if (ix, iy) in seen:
+            continue
+        seen.add((ix, iy))
+        out.append((ix, iy))
+    return np.array(out, np.int32).T.copy()
+
+
+# ----------------------------------------------------------------------------
+def plain_elastic(seed: int = 0, nt: int = 2000, nx: int = 400, ny: int = 160):
+    """Plain elastic P-SV case (400 x 160, FDORDER 4 Taylor).  Returns
+    (params, true_model, start_model, list of per-shot Geometry)."""
+    p = ShotParams(nx=nx, ny=ny, nt=nt, dh=1.0, fdorder=4, maxrelerror=0, fw=20, free_surf=1,
+                   boundary=0, vppml=1800.0, fpml=40.0, npower=2.0, k_max_pml=1.0, L=0,
+                   wavetype=1, seismo=1, source_type=1, adjoint_type=1, dtinv=2, source_shape=1)
+    rng = np.random.default_rng(seed)
+    j = np.arange(1, ny + 1, dtype=np.float64)[:, None]
+    vp_bg = (1800.0 + 1000.0 * (j - 1) / (ny - 1)) * np.ones((1, nx))
+    vs_bg = vp_bg / 1.73
+    rho = gardner_rho(vp_bg.astype(np.float32))
+    rad = 15 if (nx, ny) == (400, 160) else max(3, min(15, ny // 6))
+    lo_x, hi_x = p.fw + rad + 1, nx - p.fw - rad - 1
+    lo_z, hi_z = rad + 4, ny - p.fw - rad - 1
+    cx = rng.integers(lo_x, hi_x + 1) if hi_x > lo_x else nx // 2
+    cz = rng.integers(lo_z, hi_z + 1) if hi_z > lo_z else ny // 2
+    ii = np.arange(1, nx + 1)[None, :]
+    inside = (ii - cx) ** 2 + (j - cz) ** 2 <= rad ** 2
+    vp_t = np.where(inside, vp_bg * 1.10, vp_bg)
+    vs_t = np.where(inside, vs_bg * 1.10, vs_bg)
+    true = {"vp": vp_t.astype(np.float32), "vs": vs_t.astype(np.float32), "rho": rho.copy()}
+    start = {"vp": vp_bg.astype(np.float32), "vs": vs_bg.astype(np.float32), "rho": rho.copy()}
+    vmax = float(max(true["vp"].max(), start["vp"].max()))
+    p.dt = cfl_dt(p.dh, vmax, sum(abs(c) for c in _TAYLOR[4]))
+    xs = np.linspace(25, 375, 8) * nx / 400.0
+    xr = np.linspace(22, 378, 100) * nx / 400.0
+    rec = receiver_rows(p, xr * p.dh, np.full(xr.shape, 3 * p.dh))
+    geoms = [Geometry(source_rows(p, x * p.dh, 3 * p.dh, fc=40.0), rec) for x in xs]
+    return p, true, start, geoms
+
+
+def qfit_tau(L: int, q: float, f1: float, f2: float, nfreq: int = 400):
+    """tau-method constant-Q fit (Blanch, Robertsson & Symes 1995): relaxation
+    frequencies log-spaced over [f1, f2]; tau minimises
+    int (tau * S(w) - 1/Q)^2 dw with S(w) = sum_l w t_l / (1 + w^2 t_l^2)."""
+    fl = np.geomspace(f1, f2, L) if L > 1 else np.array([math.sqrt(f1 * f2)])
+    tl = 1.0 / (2.0 * np.pi * fl)
+    w = 2.0 * np.pi * np.linspace(f1, f2, nfreq)
+    S = np.sum(w[:, None] * tl[None, :] / (1.0 + (w[:, None] * tl[None, :]) ** 2), axis=1)
+    tau = (1.0 / q) * S.sum() / (S * S).sum()
+    return [float(np.float32(f)) for f in fl], float(np.float32(tau))
+
+
+def layered_faulted(rng, nx, ny, nlayers, vmin, vmax, nfaults, dh):
+    """Layer-cake velocity with seeded thicknesses, increasing with depth, cut
+    by seeded dipping normal faults that offset the layers."""
+    cuts = np.sort(rng.uniform(0.05, 0.95, nlayers - 1)) * ny
+    tops = np.concatenate([[0.0], cuts])
+    vels = np.sort(rng.uniform(vmin, vmax, nlayers))
+    vels[0], vels[-1] = vmin, vmax
+    jj = np.arange(ny, dtype=np.float64)[:, None] * np.ones((1, nx))
+    shift = np.zeros((ny, nx))
+    ii = np.arange(nx, dtype=np.float64)[None, :] * np.ones((ny, 1))
+    for _ in range(nfaults):
+        x0 = rng.uniform(0.15, 0.85) * nx
+        dip = math.radians(rng.uniform(50.0, 75.0))
+        throw = rng.uniform(0.02, 0.06) * ny
+        hanging = ii > x0 + jj / math.tan(dip)
+        shift = shift + np.where(hanging, throw, 0.0)
+    depth = np.clip(jj - shift, 0, ny - 1)
+    idx = np.searchsorted(tops, depth, side="right") - 1
+    return vels[np.clip(idx, 0, nlayers - 1)].astype(np.float32)
+
+
+def visco_layered(seed: int = 0, nt: int = 6000, nx: int = 2000, ny: int = 600, nshots: int = 64, ntr: int = 400):
+    """Viscoelastic P-SV case (2000 x 600, FDORDER 8 Holberg 0.1 %, L=3,
+    Q=20 over 5-60 Hz).  Returns (params, model, list of Geometry)."""
+    fl, tau = qfit_tau(3, 20.0, 5.0, 60.0)
+    p = ShotParams(nx=nx, ny=ny, nt=nt, dh=2.0, fdorder=8, maxrelerror=1, fw=30, free_surf=1,
+                   boundary=0, vppml=1500.0, fpml=15.0, npower=2.0, k_max_pml=1.0, L=3, fl=fl, tau=tau,
+                   f_ref=15.0, wavetype=1, seismo=1, source_type=1, adjoint_type=1, dtinv=3, source_shape=1)
+    rng = np.random.default_rng(seed)
+    vp = layered_faulted(rng, nx, ny, 12, 1500.0, 4500.0, 3, p.dh)
+    model = {"vp": vp, "vs": (vp / np.float32(1.73)).astype(np.float32), "rho": gardner_rho(vp)}
+    # the unrelaxed (high-frequency) velocity sets the stability limit
+    vmax = float(vp.max()) * math.sqrt(1.0 + p.L * tau)
+    p.dt = cfl_dt(p.dh, vmax, sum(abs(c) for c in _HOLBERG_01[8]))
+    margin = p.fw + 5
+    xs = np.linspace(margin, nx - margin, nshots)
+    xr = np.linspace(margin, nx - margin, ntr)
+    rec = receiver_rows(p, xr * p.dh, np.full(xr.shape, 3 * p.dh))
+    geoms = [Geometry(source_rows(p, x * p.dh, 3 * p.dh, fc=15.0), rec) for x in xs]
+    return p, model, geoms
+
+
+def perturbations(start: dict, seed: int, count: int = 4, nx=None, ny=None):
+    """``count`` seeded perturbations of a model: one random circular
+    anomaly each (radius 8-20 cells, +-5..10 % on vp and vs)."""
+    rng = np.random.default_rng(seed)
+    ny, nx = start["vp"].shape
+    out = []
+    j = np.arange(1, ny + 1)[:, None]
+    i = np.arange(1, nx + 1)[None, :]
+    for _ in range(count):
+        r = rng.integers(8, 21)
+        cx, cz = rng.integers(40, nx - 40), rng.integers(20, max(21, ny - 30))
+        amp = rng.choice([-1.0, 1.0]) * rng.uniform(0.05, 0.10)
+        inside = (i - cx) ** 2 + (j - cz) ** 2 <= r * r
+        m = {k: v.copy() for k, v in start.items()}
+        m["vp"] = np.where(inside, m["vp"] * (1 + amp), m["vp"]).astype(np.float32)
+        m["vs"] = np.where(inside, m["vs"] * (1 + amp), m["vs"]).astype(np.float32)
+        out.append(m)
+    return out
+
+
+def batched_perturbed(seed: int = 0, nshots: int = 256, nt: int = 2000):
+    """Batched case: ``nshots`` shots round-robin over the plain_elastic start
+    model and 4 seeded perturbations, sources at linspace(25,375,nshots)."""
+    p, true, start, geoms = plain_elastic(seed, nt=nt)
+    models = [start] + perturbations(start, seed + 1, 4)
+    xs = np.linspace(25, 375, nshots)
+    rec = geoms[0].recpos
+    shots = [(k % len(models), Geometry(source_rows(p, x * p.dh, 3 * p.dh, fc=40.0), rec))
+             for k, x in enumerate(xs)]
+    return p, true, models, shots
+
+
+def gaussian_random_field(rng, nx, ny, corr_cells):
+    """Unit-variance Gaussian random field: white noise filtered in the
+    Fourier domain by a Gaussian kernel of the given correlation length."""
+    w = rng.standard_normal((ny, nx))
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.fftfreq(nx)[None, :]
+    filt = np.exp(-0.5 * (2 * np.pi) ** 2 * (kx ** 2 + ky ** 2) * (corr_cells ** 2) / 2.0)
+    f = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+    f = (f - f.mean()) / f.std()
+    return np.clip(f, -3.0, 3.0)
+
+
+def precision_layered(seed: int = 0, nt: int = 8000, nx: int = 4000, ny: int = 1200, nshots: int = 128,
+                      wavetype: int = 1, dtinv: int = 20, fc: float = 10.0):
+    """Precision case (4000 x 1200, DH 2.5 m, FDORDER 8 Holberg 0.1 %).
+    DTINV=20 keeps one snapshot every 20*dt (~3 ms), far below the Nyquist
+    interval of a 10 Hz Ricker (fmax ~ 30 Hz -> 16 ms)."""
+    p = ShotParams(nx=nx, ny=ny, nt=nt, dh=2.5, fdorder=8, maxrelerror=1, fw=30, free_surf=1, boundary=0,
+                   vppml=1500.0, fpml=fc, npower=2.0, k_max_pml=1.0, L=0, wavetype=wavetype, seismo=1,
+                   source_type=1 if wavetype == 1 else 2, adjoint_type=1, dtinv=dtinv, source_shape=1)
+    rng = np.random.default_rng(seed)
+    vp = layered_faulted(rng, nx, ny, 12, 1500.0, 5500.0, 3, p.dh)
+    g = gaussian_random_field(rng, nx, ny, 50.0 / p.dh)
+    vp = (vp * (1.0 + 0.15 * g)).astype(np.float32)
+    model = {"vp": vp, "vs": (vp / np.float32(1.73)).astype(np.float32), "rho": gardner_rho(vp)}
+    p.dt = cfl_dt(p.dh, float(vp.max()), sum(abs(c) for c in _HOLBERG_01[8]))
+    margin = p.fw + 5
+    xs = np.linspace(margin, nx - margin, nshots)
+    xr = np.linspace(margin, nx - margin, 400)
+    rec = receiver_rows(p, xr * p.dh, np.full(xr.shape, 3 * p.dh))
+    geoms = [Geometry(source_rows(p, x * p.dh, 3 * p.dh, fc=fc), rec) for x in xs]
+    return p, model, geoms
+
+
+def ricker(p: ShotParams, srcpos: np.ndarray) -> np.ndarray:
+    """Ricker signals as src/wavelet.c:67-71 evaluates them (float t, double
+    intermediates), nsrc x NT."""
+    nsrc = srcpos.shape[1]
+    out = np.zeros((nsrc, p.nt), np.float32)
+    dt = np.float32(p.dt)
+    t = (np.arange(1, p.nt + 1, dtype=np.float32) * dt).astype(np.float32)
+    for k in range(nsrc):
+        tshift, fc, a = np.float32(srcpos[3, k]), np.float32(srcpos[4, k]), np.float32(srcpos[5, k])
+        ts = np.float32(1.0 / np.float64(fc))
+        tau = (np.pi * (t.astype(np.float64) - 1.5 * np.float64(ts) - np.float64(tshift)) / np.float64(ts))
+        tau = tau.astype(np.float32)
+        tt = (-tau * tau).astype(np.float32)
+        amp = ((1.0 - 2.0 * tau.astype(np.float64) * tau.astype(np.float64)) * np.exp(tt.astype(np.float64)))
+        out[k] = (amp.astype(np.float32) * a).astype(np.float32)
+    return out
+
+
+def write_model(model: dict, prefix: str) -> None:
+    """Write vp/vs/rho as the reference reads them: raw float32, x outer,
+    y inner (src/readmod_elastic.c loop order)."""
+    for key in ("vp", "vs", "rho"):
+        np.ascontiguousarray(model[key].T, dtype=np.float32).tofile(f"{prefix}.{key}")
+
+
+def read_model(prefix: str, nx: int, ny: int) -> dict:
+    out = {}
+    for key in ("vp", "vs", "rho"):
+        a = np.fromfile(f"{prefix}.{key}", dtype=np.float32, count=nx * ny)
+        out[key] = np.ascontiguousarray(a.reshape(nx, ny).T)
+    return out
