@@ -1,0 +1,253 @@
+// Snapshot store, zero-lag correlation, gradient assembly and FP64
+// reductions of the shot solver.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "ifos_kernels.cuh"
+
+namespace ifos {
+
+// snapshot component lists: P-SV elastic (vxp1, vyp1, sxx, syy, sxy), acoustic
+// (vxp1, vyp1, sp), SH (vzp1, sxz, syz) -- the arrays copied at
+// src/IFOS2D.c:1805-1871
+struct KSnap {
+    void *base;            // slot 0, slot 0 snapshot
+    long long slot_bytes;  // bytes between slots
+    long long snap_bytes;  // bytes between snapshots of one slot
+    float *scale;          // [slot][snap][comp] absmax (low-precision formats)
+    int ncomp, ntdtinv, format;
+    int comp_plane[8];     // state plane of every component
+    long long n;           // NX*NY
+};
+
+template <typename T>
+__device__ inline T snap_load(const KSnap &s, int slot, int snap, int k, long long q) {
+    const char *b = (const char *)s.base + slot * s.slot_bytes + snap * s.snap_bytes;
+    if (s.format == 0) return ((const T *)b)[k * s.n + q];
+    const float sc = s.scale[((long long)slot * s.ntdtinv + snap) * s.ncomp + k];
+    if (s.format == 1) return (T)(__bfloat162float(((const __nv_bfloat16 *)b)[k * s.n + q]) * sc);
+    return (T)(__half2float(((const __half *)b)[k * s.n + q]) * sc);
+}
+
+// fp32/fp64 snapshot copy (one thread per cell, all components)
+template <typename T>
+__global__ void k_snap_store(KGrid g, KState<T> S, KSnap sn, int hin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx || j > g.ny) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1);
+    T *b = (T *)((char *)sn.base + slot * sn.slot_bytes + hin * sn.snap_bytes);
+    for (int k = 0; k < sn.ncomp; k++) b[k * sn.n + q] = fieldp(S, slot, sn.comp_plane[k])[c];
+}
+
+// low-precision snapshots, pass 1: absolute maximum of every component
+template <typename T>
+__global__ void k_snap_absmax(KGrid g, KState<T> S, KSnap sn, int hin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    const bool in = i <= g.nx && j <= g.ny;
+    const long long c = in ? pidx(g, j, i) : 0;
+    for (int k = 0; k < sn.ncomp; k++) {
+        float v = in ? fabsf((float)fieldp(S, slot, sn.comp_plane[k])[c]) : 0.0f;
+        for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && v > 0.0f)
+            atomicMax((unsigned int *)&sn.scale[((long long)slot * sn.ntdtinv + hin) * sn.ncomp + k],
+                      __float_as_uint(v));
+    }
+}
+
+// low-precision snapshots, pass 2: scaled conversion (round to nearest even)
+template <typename T>
+__global__ void k_snap_quant(KGrid g, KState<T> S, KSnap sn, int hin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx || j > g.ny) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1);
+    char *b = (char *)sn.base + slot * sn.slot_bytes + hin * sn.snap_bytes;
+    for (int k = 0; k < sn.ncomp; k++) {
+        const float sc = sn.scale[((long long)slot * sn.ntdtinv + hin) * sn.ncomp + k];
+        const float inv = sc > 0.0f ? 1.0f / sc : 0.0f;
+        const float v = (float)fieldp(S, slot, sn.comp_plane[k])[c] * inv;
+        if (sn.format == 1) ((__nv_bfloat16 *)b)[k * sn.n + q] = __float2bfloat16_rn(v);
+        else ((__half *)b)[k * sn.n + q] = __float2half_rn(v);
+    }
+}
+
+// gradient accumulators per slot: 5 planes of NX*NY (lam', mu', rho', mu_z', rho_z')
+struct KGrad {
+    float *acc;             // slot * 5 * n
+    float *out;             // slot * 10 * n (IFOS_G_* planes)
+    long long n;
+};
+
+// zero-lag correlation with the stored forward wavefield (src/IFOS2D.c:2379-2419)
+template <typename T>
+__global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad gr, int snap, int psv, int sh,
+                            int acoustic) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx || j > g.ny) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1);
+    float *acc = gr.acc + (long long)slot * 5 * gr.n;
+    int k = 0;
+    if (psv) {
+        const T frx = snap_load<T>(sn, slot, snap, k++, q), fry = snap_load<T>(sn, slot, snap, k++, q);
+        acc[2 * gr.n + q] += (float)((fieldp(S, slot, P_VXP1)[c] * frx) + (fieldp(S, slot, P_VYP1)[c] * fry));
+        if (!acoustic) {
+            const T fx = snap_load<T>(sn, slot, snap, k++, q), fy = snap_load<T>(sn, slot, snap, k++, q),
+                    fu = snap_load<T>(sn, slot, snap, k++, q);
+            const T sxx = fieldp(S, slot, P_SXX)[c], syy = fieldp(S, slot, P_SYY)[c], sxy = fieldp(S, slot, P_SXY)[c];
+            acc[q] += (float)((fx + fy) * (sxx + syy));
+            const T mm = modelp(M, slot, M_MM)[c], ll = modelp(M, slot, M_LL)[c];
+            if (mm != (T)0) {
+                const double t1 = (1.0 / (double)mm) * (double)(fu * sxy);
+                const double t2 = (.25 * (double)(fx + fy * (sxx + syy))) / (double)ll;
+                const double t3 = (.25 * (double)(fx - fy * (sxx - syy))) / (double)mm;
+                acc[gr.n + q] = (float)((double)acc[gr.n + q] + ((t1 + t2) + t3));
+            }
+        } else {
+            const T fp = snap_load<T>(sn, slot, snap, k++, q);
+            acc[q] += (float)((fp) * (fieldp(S, slot, P_SP)[c]));
+        }
+    }
+    if (sh) {
+        const T frz = snap_load<T>(sn, slot, snap, k++, q), fxz = snap_load<T>(sn, slot, snap, k++, q),
+                fyz = snap_load<T>(sn, slot, snap, k++, q);
+        acc[4 * gr.n + q] += (float)(fieldp(S, slot, P_VZP1)[c] * frz);
+        const T *rho = modelp(M, slot, M_RHO), *u = modelp(M, slot, M_VS);
+        const T muss = rho[c] * u[c] * u[c];
+        acc[3 * gr.n + q] = (float)((double)acc[3 * gr.n + q] +
+                                    (1.0 / (double)(muss * muss)) *
+                                        (double)(fxz * fieldp(S, slot, P_SXZ)[c] + fyz * fieldp(S, slot, P_SYZ)[c]));
+    }
+}
+
+// per-shot gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2477-2601)
+template <typename T>
+__global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int acoustic) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx || j > g.ny) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1), n = gr.n;
+    const float *acc = gr.acc + (long long)slot * 5 * n;
+    float *o = gr.out + (long long)slot * 10 * n;
+    const float wl = acc[q], wm = acc[n + q], wr = acc[2 * n + q], wmz = acc[3 * n + q], wrz = acc[4 * n + q];
+    o[0 * n + q] = wl;
+    o[1 * n + q] = wm;
+    o[2 * n + q] = wr;
+    o[6 * n + q] = wmz;
+    o[7 * n + q] = wrz;
+    const float DT = g.dt;
+    const float rho = (float)modelp(M, slot, M_RHO)[c], u = (float)modelp(M, slot, M_VS)[c],
+                pi = (float)modelp(M, slot, M_VP)[c];
+    float vp_g = 0, vs_g = 0, rho_g = 0;
+    if (psv) {
+        float lam = -DT * wl, mu = 0;
+        const float muss = !acoustic ? rho * u * u : 0;
+        const float lamss = (float)((double)(rho * pi * pi) - 2.0 * (double)muss);
+        if (!acoustic) lam = (float)((1.0 / (4.0 * (double)(lamss + muss) * (double)(lamss + muss))) * (double)lam);
+        else lam = (float)((1.0 / (double)((lamss + muss) * (lamss + muss))) * (double)lam);
+        vp_g = (float)(2.0 * (double)pi * (double)rho * (double)lam);
+        if (!acoustic) {
+            mu = -DT * wm;
+            vs_g = (float)(-4.0 * (double)rho * (double)u * (double)lam + 2.0 * (double)rho * (double)u * (double)mu);
+        } else {
+            vs_g = wm;
+        }
+        const float rho_s = -DT * wr;
+        if (!acoustic)
+            rho_g = (float)(((double)(pi * pi) - (2.0 * (double)u * (double)u)) * (double)lam +
+                            (double)(u * u * mu) + (double)rho_s);
+        else
+            rho_g = ((pi * pi) * lam) + rho_s;
+    }
+    o[3 * n + q] = vp_g;
+    o[4 * n + q] = vs_g;
+    o[5 * n + q] = rho_g;
+    if (sh && !acoustic) {
+        const float mu_z = -DT * wmz;
+        o[8 * n + q] = (float)(2.0 * (double)rho * (double)u * (double)mu_z);
+        const float rho_s_z = -DT * wrz;
+        o[9 * n + q] = ((u * u * mu_z) + rho_s_z);
+    } else {
+        o[8 * n + q] = wmz;
+        o[9 * n + q] = wrz;
+    }
+}
+
+// sum of the assembled gradients over slots (src/IFOS2D.c:2703-2724), in slot
+// order so the float additions match the reference's shot loop
+__global__ void k_grad_sum(const float *grads, int nshots, long long n, float *out) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int planes[5] = {3, 4, 5, 8, 9};
+    for (int k = 0; k < 5; k++) {
+        float s = 0.0f;
+        for (int sl = 0; sl < nshots; sl++) s += grads[(long long)sl * 10 * n + planes[k] * n + q];
+        out[k * n + q] = s;
+    }
+}
+
+// FP64 dot product, pass 1: one double partial per block (deterministic)
+__global__ void k_dot_partial(const float *a, const float *b, long long n, double *partial) {
+    double acc = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const double x = a[k];
+        acc += x * (b ? (double)b[k] : x);
+    }
+    __shared__ double red[32];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+// pass 2: fixed-order sum of the partials
+__global__ void k_dot_final(const double *partial, int nb, double *out) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += partial[k];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) *out = v;
+    }
+}
+
+// residuals of one component, LNORM=2, VELOCITY=0 (src/calc_res.c:137-281):
+// per trace, running float sums times DT, time-reversed difference; the
+// misfit and energy partial sums per trace in double
+__global__ void k_calc_res(const float *obs, const float *syn, float *diff, int ntr, int ns, float dt,
+                           double *l2_tr, double *en_tr) {
+    const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tr >= ntr) return;
+    const float *s = syn + (long long)tr * ns, *d = obs + (long long)tr * ns;
+    float *df = diff + (long long)tr * ns;
+    float rs = 0.0f, rd = 0.0f;
+    double l2 = 0.0, en = 0.0;
+    for (int j = 0; j < ns; j++) {
+        rs += s[j];
+        rd += d[j];
+        const float is = rs * dt, id = rd * dt;
+        const float r = is - id;
+        df[ns - 1 - j] = r;
+        l2 += (double)r * (double)r;
+        en += (double)id * (double)id;
+    }
+    l2_tr[tr] = l2;
+    en_tr[tr] = en;
+}
+
+}  // namespace ifos

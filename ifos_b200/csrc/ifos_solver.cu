@@ -1,0 +1,990 @@
+// libifos_b200: device context, time loops and the C ABI (include/ifos_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ifos_gpu.h"
+#include "ifos_kernels.cuh"
+#include "ifos_setup.h"
+#include "ifos_snap.cuh"
+
+using namespace ifos;
+
+namespace {
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+}  // namespace
+
+struct ifos_ctx {
+    ifos_params p{};
+    int device = 0;
+    bool dbl = false;  // fp64 arithmetic
+    size_t esz = 4;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    KGrid g{};
+    int psv = 0, sh = 0, ac = 0;
+    // state
+    DevBuf state, psi, models, prof, srf, slot_model, src_pos, src_sig, src_n, rec_pos, rec_n, adj, sec, snap,
+        snap_scale, gacc, gout, bad, dot_partial, dot_out, res_tr;
+    long long slot_stride = 0, psix_len = 0, psiy_len = 0, psi_slot = 0, model_stride = 0;
+    long long off[NP_FIELD];
+    long long mem_off[5];
+    bool mplane[NM_PLANE];
+    long long moff[NM_PLANE];
+    bool tau_planes = false;
+    ViscoScalars vsc{};
+    // snapshots
+    bool with_snap = false;
+    int ncomp = 0, comp_plane[8] = {0};
+    long long snap_bytes = 0, snap_slot_bytes = 0;
+    bool snaps_valid = false;
+    int fwd_nshots = 0;
+    // host mirrors
+    std::vector<int> nsrc_h, ntr_h, slot_model_h;
+    std::vector<float> srcpos_h;
+    bool adj_staged = false;
+    float last_ms = 0.0f;
+    long long launches = 0;
+};
+
+// ----------------------------------------------------------------------------
+static int fail(ifos_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+#define CK(call)                                                                                            \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) return fail(c, IFOS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static int dev_alloc(ifos_ctx *c, DevBuf &b, size_t bytes) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    if (!bytes) return IFOS_OK;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return fail(c, IFOS_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return IFOS_OK;
+}
+static void dev_free(DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+static int check_params(const ifos_params &p, std::string &why) {
+    auto bad = [&](const char *m) {
+        why = m;
+        return IFOS_ERR_ARG;
+    };
+    if (p.nx < 1 || p.ny < 1 || p.nt < 1) return bad("NX, NY and NT must be positive");
+    if (p.fdorder < 2 || p.fdorder > 12 || (p.fdorder & 1)) return bad("FDORDER must be 2, 4, 6, 8, 10 or 12");
+    if (p.maxrelerror < 0 || p.maxrelerror > 4) return bad("MAXRELERROR must be 0..4");
+    if (p.fw < 0 || 2 * p.fw > p.nx || 2 * p.fw > p.ny) return bad("FW does not fit the grid");
+    if (p.L < 0 || p.L > IFOS_MAX_L) return bad("L must be 0..8");
+    if (p.wavetype < 1 || p.wavetype > 3) return bad("WAVETYPE must be 1, 2 or 3");
+    if (p.acoustic && p.wavetype != 1) return bad("acoustic modelling is P-SV only");
+    if (p.acoustic && p.L) return bad("viscoacoustic modelling is not implemented on the device");
+    if (p.parameterization != 1) return bad("only PARAMETERIZATION=1 is implemented");
+    if (p.velocity != 0) return bad("only VELOCITY=0 is implemented");
+    if (p.dtinv < 1 || p.nt % p.dtinv) return bad("NT must be a multiple of DTINV");
+    if (p.seismo < 0 || p.seismo > 5) return bad("SEISMO must be 0..5");
+    if (p.max_shots < 1 || p.max_models < 1) return bad("max_shots and max_models must be >= 1");
+    if (p.max_src < 0 || p.max_rec < 0) return bad("max_src/max_rec must be >= 0");
+    if (p.snap_format < 0 || p.snap_format > 2) return bad("snap_format must be 0, 1 or 2");
+    if (p.precision < 0 || p.precision > 1) return bad("precision must be 0 or 1");
+    if (!(p.dt > 0) || !(p.dh > 0)) return bad("DT and DH must be positive");
+    for (int l = 0; l < p.L; l++)
+        if (!(p.fl[l] > 0)) return bad("FL1..FLL must be positive");
+    return IFOS_OK;
+}
+
+struct Layout {
+    long long pitch, rows, plane, slot_elems, psix, psiy, psi_slot, model_elems;
+    int nfield, nmem, nmodel;
+    long long snap_bytes_per, snap_slot_bytes;
+    int ncomp;
+};
+
+static Layout layout_of(const ifos_params &p) {
+    Layout L{};
+    L.pitch = ((p.nx + 2 * HX) + 31) / 32 * 32;
+    L.rows = p.ny + 2 * HY;
+    L.plane = L.pitch * L.rows;
+    const int psv = p.wavetype != 2, sh = p.wavetype != 1;
+    L.nfield = 0;
+    if (psv) L.nfield += p.acoustic ? 5 : 7;
+    if (sh) L.nfield += 4;
+    L.nmem = p.L ? (psv ? 3 * p.L : 0) + (sh ? 2 * p.L : 0) : 0;
+    L.slot_elems = (long long)(L.nfield + L.nmem) * L.plane;
+    L.psix = (long long)p.ny * 2 * p.fw;
+    L.psiy = (long long)2 * p.fw * p.nx;
+    L.psi_slot = NX_STRIP * L.psix + NY_STRIP * L.psiy;
+    // model planes: rho vp vs rip rjp always; + elastic (uipjp f g mm ll) or acoustic g;
+    // + visco (fipjp f g mu pi muipjp [taus taup tausipjp])
+    L.nmodel = 5 + (p.acoustic ? 1 : 5) + (p.L ? 9 : 0);
+    L.model_elems = (long long)L.nmodel * L.plane;
+    L.ncomp = (psv ? (p.acoustic ? 3 : 5) : 0) + (sh ? 3 : 0);
+    const int bytes = p.snap_format == 0 ? (p.precision ? 8 : 4) : 2;
+    L.snap_bytes_per = (long long)L.ncomp * p.nx * p.ny * bytes;
+    L.snap_slot_bytes = L.snap_bytes_per * (p.nt / p.dtinv);
+    return L;
+}
+
+extern "C" void ifos_params_default(ifos_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->nx = 100;
+    p->ny = 100;
+    p->nt = 1000;
+    p->dh = 1.0f;
+    p->dt = 1e-4f;
+    p->fdorder = 4;
+    p->fw = 10;
+    p->free_surf = 1;
+    p->vppml = 1800.0f;
+    p->fpml = 20.0f;
+    p->npower = 2.0f;
+    p->k_max_pml = 1.0f;
+    p->wavetype = 1;
+    p->parameterization = 1;
+    p->seismo = 1;
+    p->source_type = 1;
+    p->adjoint_type = 1;
+    p->dtinv = 1;
+    p->max_shots = 1;
+    p->max_models = 1;
+    p->max_src = 1;
+    p->max_rec = 1;
+}
+
+extern "C" size_t ifos_ctx_bytes(const ifos_params *p, int with_snapshots) {
+    if (!p) return 0;
+    Layout L = layout_of(*p);
+    const size_t e = p->precision ? 8 : 4;
+    size_t b = (size_t)p->max_shots * (L.slot_elems + L.psi_slot) * e;
+    b += (size_t)p->max_models * (L.model_elems * e + 4 * (size_t)p->nx * e);
+    b += (size_t)p->max_shots * ((size_t)8 * p->max_src * 4 + (size_t)p->max_src * p->nt * 4 + (size_t)2 * p->max_rec * 4 +
+                                 (size_t)3 * p->max_rec * p->nt * 4 + (size_t)IFOS_NS * p->max_rec * p->nt * 4);
+    b += (size_t)p->max_shots * (size_t)15 * p->nx * p->ny * 4;
+    if (with_snapshots) b += (size_t)p->max_shots * L.snap_slot_bytes;
+    return b;
+}
+
+extern "C" const char *ifos_last_error(const ifos_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
+    if (!c) return IFOS_OK;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    DevBuf *bufs[] = {&c->state, &c->psi, &c->models, &c->prof, &c->srf, &c->slot_model, &c->src_pos, &c->src_sig,
+                      &c->src_n, &c->rec_pos, &c->rec_n, &c->adj, &c->sec, &c->snap, &c->snap_scale, &c->gacc,
+                      &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
+    for (DevBuf *b : bufs) dev_free(*b);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return IFOS_OK;
+}
+
+extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snapshots, ifos_ctx **out) {
+    ifos_ctx *c = nullptr;
+    if (!pp || !out) return fail(c, IFOS_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    if (int rc = check_params(*pp, why)) return fail(c, rc, why);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(c, IFOS_ERR_CUDA, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(c, IFOS_ERR_ARG, "bad device index");
+    c = new (std::nothrow) ifos_ctx();
+    if (!c) return fail(nullptr, IFOS_ERR_NOMEM, "host allocation failed");
+    c->p = *pp;
+    c->device = device;
+    const ifos_params &p = c->p;
+    c->dbl = p.precision == 1;
+    c->esz = c->dbl ? 8 : 4;
+    c->psv = p.wavetype != 2;
+    c->sh = p.wavetype != 1;
+    c->ac = p.acoustic;
+    c->with_snap = with_snapshots != 0;
+    auto bail = [&](int rc) {
+        g_create_error = c->err;
+        ifos_ctx_destroy(c);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+        return bail(fail(c, IFOS_ERR_CUDA, "stream/event creation failed"));
+
+    Layout L = layout_of(p);
+    KGrid &g = c->g;
+    g.nx = p.nx;
+    g.ny = p.ny;
+    g.pitch = (int)L.pitch;
+    g.plane = L.plane;
+    g.fw = p.fw;
+    g.free_surf = p.free_surf;
+    g.boundary = p.boundary;
+    g.fdoh = p.fdorder / 2;
+    g.L = p.L;
+    g.quirk_hi = (p.fdorder >= 10 && !p.hi_order_corrected && (c->psv || c->ac)) ? 1 : 0;
+    g.nt_total = p.nt;
+    g.dt = p.dt;
+    g.dh = p.dh;
+    g.adjoint_type = p.adjoint_type;
+    if (!fd_coefficients(p.fdorder, p.maxrelerror, g.hc)) return bail(fail(c, IFOS_ERR_ARG, "bad FD order"));
+    c->vsc = visco_scalars(p);
+    for (int l = 0; l <= IFOS_MAX_L; l++) {
+        g.eta[l] = c->vsc.eta[l];
+        g.bip[l] = c->vsc.bip[l];
+        g.bjm[l] = c->vsc.bjm[l];
+        g.cip[l] = c->vsc.cip[l];
+        g.cjm[l] = c->vsc.cjm[l];
+        g.bjm_srf[l] = c->vsc.bjm_srf[l];
+    }
+
+    // state plane table
+    for (auto &o : c->off) o = -1;
+    for (auto &o : c->mem_off) o = -1;
+    long long k = 0;
+    if (c->psv) {
+        c->off[P_VX] = k++ * L.plane;
+        c->off[P_VY] = k++ * L.plane;
+        if (!c->ac) {
+            c->off[P_SXX] = k++ * L.plane;
+            c->off[P_SYY] = k++ * L.plane;
+            c->off[P_SXY] = k++ * L.plane;
+        } else {
+            c->off[P_SP] = k++ * L.plane;
+        }
+        c->off[P_VXP1] = k++ * L.plane;
+        c->off[P_VYP1] = k++ * L.plane;
+    }
+    if (c->sh) {
+        c->off[P_VZ] = k++ * L.plane;
+        c->off[P_SXZ] = k++ * L.plane;
+        c->off[P_SYZ] = k++ * L.plane;
+        c->off[P_VZP1] = k++ * L.plane;
+    }
+    if (p.L) {
+        if (c->psv)
+            for (int w = 0; w < 3; w++) {
+                c->mem_off[w] = k * L.plane;
+                k += p.L;
+            }
+        if (c->sh)
+            for (int w = 3; w < 5; w++) {
+                c->mem_off[w] = k * L.plane;
+                k += p.L;
+            }
+    }
+    c->slot_stride = L.slot_elems;
+    c->psix_len = L.psix;
+    c->psiy_len = L.psiy;
+    c->psi_slot = L.psi_slot;
+    // snapshot components
+    c->ncomp = 0;
+    if (c->psv) {
+        c->comp_plane[c->ncomp++] = P_VXP1;
+        c->comp_plane[c->ncomp++] = P_VYP1;
+        if (!c->ac) {
+            c->comp_plane[c->ncomp++] = P_SXX;
+            c->comp_plane[c->ncomp++] = P_SYY;
+            c->comp_plane[c->ncomp++] = P_SXY;
+        } else {
+            c->comp_plane[c->ncomp++] = P_SP;
+        }
+    }
+    if (c->sh) {
+        c->comp_plane[c->ncomp++] = P_VZP1;
+        c->comp_plane[c->ncomp++] = P_SXZ;
+        c->comp_plane[c->ncomp++] = P_SYZ;
+    }
+    c->snap_bytes = L.snap_bytes_per;
+    c->snap_slot_bytes = L.snap_slot_bytes;
+
+    const size_t e = c->esz;
+    const int S = p.max_shots;
+    int rc = IFOS_OK;
+    if ((rc = dev_alloc(c, c->state, (size_t)S * L.slot_elems * e))) return bail(rc);
+    if ((rc = dev_alloc(c, c->psi, (size_t)S * L.psi_slot * e + e))) return bail(rc);
+    c->model_stride = L.model_elems;
+    if ((rc = dev_alloc(c, c->models, (size_t)p.max_models * L.model_elems * e))) return bail(rc);
+    if ((rc = dev_alloc(c, c->prof, (size_t)12 * (2 * p.fw + 1) * e))) return bail(rc);
+    if ((rc = dev_alloc(c, c->srf, (size_t)p.max_models * 4 * p.nx * e))) return bail(rc);
+    if ((rc = dev_alloc(c, c->slot_model, (size_t)S * sizeof(int)))) return bail(rc);
+    const int ms = std::max(1, p.max_src), mr = std::max(1, p.max_rec);
+    if ((rc = dev_alloc(c, c->src_pos, (size_t)S * 8 * ms * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->src_sig, (size_t)S * ms * p.nt * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->src_n, (size_t)S * sizeof(int)))) return bail(rc);
+    if ((rc = dev_alloc(c, c->rec_pos, (size_t)S * 2 * mr * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->rec_n, (size_t)S * sizeof(int)))) return bail(rc);
+    if ((rc = dev_alloc(c, c->adj, (size_t)S * 3 * mr * p.nt * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->sec, (size_t)S * IFOS_NS * mr * p.nt * 4))) return bail(rc);
+    const long long N = (long long)p.nx * p.ny;
+    if ((rc = dev_alloc(c, c->gacc, (size_t)S * 5 * N * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->gout, (size_t)S * IFOS_NG * N * 4))) return bail(rc);
+    if ((rc = dev_alloc(c, c->bad, sizeof(int)))) return bail(rc);
+    if ((rc = dev_alloc(c, c->dot_partial, 1024 * sizeof(double)))) return bail(rc);
+    if ((rc = dev_alloc(c, c->dot_out, 2 * sizeof(double)))) return bail(rc);
+    if (c->with_snap) {
+        if ((rc = dev_alloc(c, c->snap, (size_t)S * L.snap_slot_bytes))) return bail(rc);
+        if ((rc = dev_alloc(c, c->snap_scale, (size_t)S * (p.nt / p.dtinv) * c->ncomp * sizeof(float) + 4)))
+            return bail(rc);
+    }
+    // zero everything that is read before it is written (halos stay zero)
+    DevBuf *zb[] = {&c->state, &c->psi, &c->models, &c->srf, &c->slot_model, &c->src_pos, &c->src_sig, &c->src_n,
+                    &c->rec_pos, &c->rec_n, &c->adj, &c->sec, &c->gacc, &c->gout, &c->bad};
+    for (DevBuf *b : zb)
+        if (b->p) CK(cudaMemsetAsync(b->p, 0, b->bytes, c->st));
+    // CPML profiles
+    CpmlProfiles pr = cpml_profiles(p);
+    {
+        std::vector<char> hb((size_t)12 * (2 * p.fw + 1) * e);
+        for (int a = 0; a < 12; a++)
+            for (int h = 0; h <= 2 * p.fw; h++) {
+                size_t idx = (size_t)a * (2 * p.fw + 1) + h;
+                if (c->dbl) ((double *)hb.data())[idx] = pr.arr[a][h];
+                else ((float *)hb.data())[idx] = pr.arr[a][h];
+            }
+        CK(cudaMemcpyAsync(c->prof.p, hb.data(), hb.size(), cudaMemcpyHostToDevice, c->st));
+    }
+    // model plane table
+    for (int m = 0; m < NM_PLANE; m++) {
+        c->mplane[m] = false;
+        c->moff[m] = -1;
+    }
+    std::vector<int> present = {M_RHO, M_VP, M_VS, M_RIP, M_RJP};
+    if (c->ac) present.push_back(M_GAC);
+    else {
+        present.push_back(M_UIPJP);
+        present.push_back(M_F);
+        present.push_back(M_G);
+        present.push_back(M_MM);
+        present.push_back(M_LL);
+    }
+    if (p.L)
+        for (int m : {M_FIPJPV, M_FV, M_GV, M_MUR, M_PIR, M_MUIPJPR, M_TAUS, M_TAUP, M_TAUSIPJP}) present.push_back(m);
+    for (size_t q = 0; q < present.size(); q++) {
+        c->mplane[present[q]] = true;
+        c->moff[present[q]] = (long long)q * L.plane;
+    }
+    c->nsrc_h.assign(S, 0);
+    c->ntr_h.assign(S, 0);
+    c->slot_model_h.assign(S, 0);
+    c->srcpos_h.assign((size_t)S * 8 * ms, 0.0f);
+    CK(cudaStreamSynchronize(c->st));
+    *out = c;
+    return IFOS_OK;
+}
+
+// ----------------------------------------------------------------------------
+template <typename T>
+static void upload_plane(std::vector<T> &host, const ifos_ctx *c, long long off, const std::vector<float> &src) {
+    const ifos_params &p = c->p;
+    for (int j = 1; j <= p.ny; j++)
+        for (int i = 1; i <= p.nx; i++)
+            host[off + pidx(c->g, j, i)] = (T)src[(size_t)(j - 1) * p.nx + (i - 1)];
+}
+
+template <typename T>
+static int model_upload_t(ifos_ctx *c, int model, const ModelPlanes &mp) {
+    const Layout L = layout_of(c->p);
+    std::vector<T> h((size_t)L.model_elems, (T)0);
+    auto put = [&](int id, const std::vector<float> &v) {
+        if (c->mplane[id] && !v.empty()) upload_plane<T>(h, c, c->moff[id], v);
+    };
+    put(M_RHO, mp.rho);
+    put(M_VP, mp.vp);
+    put(M_VS, mp.vs);
+    put(M_RIP, mp.rip);
+    put(M_RJP, mp.rjp);
+    put(M_UIPJP, mp.uipjp);
+    put(M_F, mp.f_el);
+    put(M_G, mp.g_el);
+    put(M_GAC, mp.g_ac);
+    put(M_MM, mp.mm);
+    put(M_LL, mp.ll);
+    put(M_FIPJPV, mp.fipjp_v);
+    put(M_FV, mp.f_v);
+    put(M_GV, mp.g_v);
+    put(M_MUR, mp.mu_r);
+    put(M_PIR, mp.pi_r);
+    put(M_MUIPJPR, mp.muipjp_r);
+    put(M_TAUS, mp.taus);
+    put(M_TAUP, mp.taup);
+    put(M_TAUSIPJP, mp.tausipjp);
+    ifos_ctx *cc = c;
+    {
+        ifos_ctx *c = cc;
+        CK(cudaMemcpyAsync((char *)c->models.p + (size_t)model * L.model_elems * sizeof(T), h.data(),
+                           h.size() * sizeof(T), cudaMemcpyHostToDevice, c->st));
+        std::vector<T> s((size_t)4 * c->p.nx, (T)0);
+        for (int i = 0; i < c->p.nx; i++) {
+            if (!mp.srf_fjm.empty()) s[i] = mp.srf_fjm[i];
+            if (!mp.srf_g.empty()) s[c->p.nx + i] = mp.srf_g[i];
+            if (!mp.srf_djm.empty()) s[2 * c->p.nx + i] = mp.srf_djm[i];
+            if (!mp.srf_e.empty()) s[3 * c->p.nx + i] = mp.srf_e[i];
+        }
+        CK(cudaMemcpyAsync((char *)c->srf.p + (size_t)model * 4 * c->p.nx * sizeof(T), s.data(), s.size() * sizeof(T),
+                           cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return IFOS_OK;
+}
+
+extern "C" int ifos_model_upload(ifos_ctx *c, int model, const float *vp, const float *vs, const float *rho,
+                                 const float *taup, const float *taus) {
+    if (!c) return IFOS_ERR_ARG;
+    if (model < 0 || model >= c->p.max_models) return fail(c, IFOS_ERR_ARG, "model index out of range");
+    ModelPlanes mp;
+    if (!build_model(c->p, vp, vs, rho, taup, taus, mp)) return fail(c, IFOS_ERR_ARG, "missing model arrays");
+    for (size_t k = 0; k < mp.rho.size(); k++)
+        if (!(mp.rho[k] > 0) || !std::isfinite(mp.vp[k]) || !std::isfinite(mp.vs[k]))
+            return fail(c, IFOS_ERR_ARG, "model has non-finite values or non-positive density");
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    if (c->p.L) {
+        // all models of a context share the tau representation of the first upload
+        if (!mp.tau_uniform) c->tau_planes = true;
+        c->g.taus0 = mp.taus0;
+        c->g.taup0 = mp.taup0;
+        c->g.tausipjp0 = mp.tausipjp0;
+        if (mp.tau_uniform) {
+            // planes stay in the table but are ignored (the kernels read the scalars)
+            mp.taus.assign(mp.rho.size(), mp.taus0);
+            mp.taup.assign(mp.rho.size(), mp.taup0);
+            mp.tausipjp.assign(mp.rho.size(), mp.tausipjp0);
+        }
+    }
+    c->snaps_valid = false;
+    return c->dbl ? model_upload_t<double>(c, model, mp) : model_upload_t<float>(c, model, mp);
+}
+
+extern "C" int ifos_shot_setup(ifos_ctx *c, int slot, int model, int nsrc, const float *srcpos, const float *signals,
+                               int ntr, const int *recpos) {
+    if (!c) return IFOS_ERR_ARG;
+    const ifos_params &p = c->p;
+    if (slot < 0 || slot >= p.max_shots) return fail(c, IFOS_ERR_ARG, "slot out of range");
+    if (model < 0 || model >= p.max_models) return fail(c, IFOS_ERR_ARG, "model out of range");
+    if (nsrc < 0 || nsrc > p.max_src) return fail(c, IFOS_ERR_ARG, "nsrc exceeds max_src");
+    if (ntr < 0 || ntr > p.max_rec) return fail(c, IFOS_ERR_ARG, "ntr exceeds max_rec");
+    if ((nsrc && (!srcpos || !signals)) || (ntr && !recpos)) return fail(c, IFOS_ERR_ARG, "null geometry");
+    for (int l = 0; l < nsrc; l++) {
+        const int i = (int)srcpos[l], j = (int)srcpos[nsrc + l];
+        if (i < 1 || i > p.nx || j < 1 || j > p.ny)
+            return fail(c, IFOS_ERR_ARG, "source " + std::to_string(l) + " outside the grid");
+    }
+    for (int l = 0; l < ntr; l++) {
+        const int i = recpos[l], j = recpos[ntr + l];
+        if (i < 1 || i > p.nx || j < 1 || j > p.ny)
+            return fail(c, IFOS_ERR_ARG, "receiver " + std::to_string(l) + " outside the grid");
+        for (int m = 0; m < l; m++)
+            if (recpos[m] == i && recpos[ntr + m] == j)
+                return fail(c, IFOS_ERR_ARG, "receivers must be unique per cell (src/receiver.c:73-88)");
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    const int ms = std::max(1, p.max_src), mr = std::max(1, p.max_rec);
+    std::vector<float> pos((size_t)8 * ms, 0.0f);
+    for (int r = 0; r < 8; r++)
+        for (int l = 0; l < nsrc; l++) pos[(size_t)r * ms + l] = srcpos[(size_t)r * nsrc + l];
+    std::vector<int> rp((size_t)2 * mr, 1);
+    for (int r = 0; r < 2; r++)
+        for (int l = 0; l < ntr; l++) rp[(size_t)r * mr + l] = recpos[(size_t)r * ntr + l];
+    CK(cudaMemcpyAsync((char *)c->src_pos.p + (size_t)slot * 8 * ms * 4, pos.data(), pos.size() * 4,
+                       cudaMemcpyHostToDevice, c->st));
+    if (nsrc)
+        CK(cudaMemcpyAsync((char *)c->src_sig.p + (size_t)slot * ms * p.nt * 4, signals, (size_t)nsrc * p.nt * 4,
+                           cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((char *)c->rec_pos.p + (size_t)slot * 2 * mr * 4, rp.data(), rp.size() * 4,
+                       cudaMemcpyHostToDevice, c->st));
+    c->nsrc_h[slot] = nsrc;
+    c->ntr_h[slot] = ntr;
+    c->slot_model_h[slot] = model;
+    std::copy(pos.begin(), pos.end(), c->srcpos_h.begin() + (size_t)slot * 8 * ms);
+    CK(cudaMemcpyAsync((char *)c->src_n.p + slot * 4, &c->nsrc_h[slot], 4, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((char *)c->rec_n.p + slot * 4, &c->ntr_h[slot], 4, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((char *)c->slot_model.p + slot * 4, &c->slot_model_h[slot], 4, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->snaps_valid = false;
+    return IFOS_OK;
+}
+
+// ----------------------------------------------------------------------------
+template <typename T>
+static KState<T> kstate(const ifos_ctx *c) {
+    KState<T> s{};
+    s.base = (T *)c->state.p;
+    s.slot_stride = c->slot_stride;
+    for (int k = 0; k < NP_FIELD; k++) s.off[k] = c->off[k] < 0 ? 0 : c->off[k];
+    for (int k = 0; k < 5; k++) s.mem_off[k] = c->mem_off[k] < 0 ? 0 : c->mem_off[k];
+    T *psi = (T *)c->psi.p;
+    for (int k = 0; k < NX_STRIP; k++) s.psix[k] = psi + k * c->psix_len;
+    for (int k = 0; k < NY_STRIP; k++) s.psiy[k] = psi + NX_STRIP * c->psix_len + k * c->psiy_len;
+    s.psix_slot = c->psi_slot;
+    s.psiy_slot = c->psi_slot;
+    return s;
+}
+template <typename T>
+static KModel<T> kmodel(const ifos_ctx *c) {
+    KModel<T> m{};
+    for (int k = 0; k < NM_PLANE; k++) {
+        bool use = c->mplane[k];
+        if ((k == M_TAUS || k == M_TAUP || k == M_TAUSIPJP) && !c->tau_planes) use = false;
+        m.m[k] = use ? (const T *)c->models.p + c->moff[k] : nullptr;
+    }
+    m.model_stride = c->model_stride;
+    m.slot_model = (const int *)c->slot_model.p;
+    m.prof = (const T *)c->prof.p;
+    m.srf = (const T *)c->srf.p;
+    m.srf_stride = 4LL * c->p.nx;
+    return m;
+}
+static KSrc ksrc(const ifos_ctx *c) {
+    KSrc s{};
+    s.pos = (const float *)c->src_pos.p;
+    s.sig = (const float *)c->src_sig.p;
+    s.nsrc = (const int *)c->src_n.p;
+    s.max_src = std::max(1, c->p.max_src);
+    s.nt_total = c->p.nt;
+    return s;
+}
+static KRec krec(const ifos_ctx *c) {
+    KRec r{};
+    r.pos = (const int *)c->rec_pos.p;
+    r.ntr = (const int *)c->rec_n.p;
+    r.max_rec = std::max(1, c->p.max_rec);
+    r.adj = (const float *)c->adj.p;
+    r.sec = (float *)c->sec.p;
+    return r;
+}
+static KSnap ksnap(const ifos_ctx *c) {
+    KSnap s{};
+    s.base = c->snap.p;
+    s.slot_bytes = c->snap_slot_bytes;
+    s.snap_bytes = c->snap_bytes;
+    s.scale = (float *)c->snap_scale.p;
+    s.ncomp = c->ncomp;
+    s.ntdtinv = c->p.nt / c->p.dtinv;
+    s.format = c->p.snap_format;
+    for (int k = 0; k < 8; k++) s.comp_plane[k] = c->comp_plane[k];
+    s.n = (long long)c->p.nx * c->p.ny;
+    return s;
+}
+
+#define DISPATCH_FDOH(fdoh, ...)                 \
+    switch (fdoh) {                              \
+        case 1: { constexpr int FD = 1; __VA_ARGS__; } break; \
+        case 2: { constexpr int FD = 2; __VA_ARGS__; } break; \
+        case 3: { constexpr int FD = 3; __VA_ARGS__; } break; \
+        case 4: { constexpr int FD = 4; __VA_ARGS__; } break; \
+        case 5: { constexpr int FD = 5; __VA_ARGS__; } break; \
+        default: { constexpr int FD = 6; __VA_ARGS__; } break; \
+    }
+
+template <typename T>
+struct Launcher {
+    ifos_ctx *c;
+    KState<T> S;
+    KModel<T> M;
+    KSrc src;
+    KRec rec;
+    dim3 blk{32, 8, 1}, grd;
+    int nshots;
+    Launcher(ifos_ctx *cc, int ns) : c(cc), nshots(ns) {
+        S = kstate<T>(c);
+        M = kmodel<T>(c);
+        src = ksrc(c);
+        rec = krec(c);
+        grd = dim3((c->p.nx + 31) / 32, (c->p.ny + 7) / 8, ns);
+    }
+    void v_step(int sw, int want_p1) {
+        const KGrid &g = c->g;
+        DISPATCH_FDOH(g.fdoh, {
+            if (c->ac) k_v_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M, sw, want_p1);
+            else {
+                if (c->psv) k_v_psv<T, FD><<<grd, blk, 0, c->st>>>(g, S, M, sw, want_p1);
+                if (c->sh) k_v_sh<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+            }
+        });
+        c->launches += (c->ac ? 1 : c->psv + c->sh);
+    }
+    void s_step() {
+        const KGrid &g = c->g;
+        DISPATCH_FDOH(g.fdoh, {
+            if (c->ac) k_p_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+            else {
+                if (c->psv) {
+                    if (g.L) k_s_psv_visc<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+                    else k_s_psv_el<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+                }
+                if (c->sh) k_s_sh<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+            }
+        });
+        c->launches += (c->ac ? 1 : c->psv + c->sh);
+    }
+    void surface() {
+        const KGrid &g = c->g;
+        dim3 gs((c->p.nx + 127) / 128, nshots);
+        DISPATCH_FDOH(g.fdoh, k_surface<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, c->psv, c->sh, c->ac));
+        c->launches++;
+    }
+    void seismo(int nt) {
+        const KGrid &g = c->g;
+        dim3 gs((std::max(1, c->p.max_rec) + 127) / 128, nshots);
+        DISPATCH_FDOH(g.fdoh, k_seismo<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, rec, nt, c->p.seismo, c->psv, c->sh,
+                                                                     c->ac, (int *)c->bad.p));
+        c->launches++;
+    }
+};
+
+static bool any_force_source(const ifos_ctx *c, int nshots) {
+    const int ms = std::max(1, c->p.max_src);
+    for (int s = 0; s < nshots; s++)
+        for (int l = 0; l < c->nsrc_h[s]; l++) {
+            int t = (int)c->srcpos_h[(size_t)s * 8 * ms + 7 * ms + l];
+            if (t == 2 || t == 3 || t == 4) return true;
+        }
+    return false;
+}
+
+template <typename T>
+static int zero_state(ifos_ctx *c, int nshots) {
+    CK(cudaMemsetAsync(c->state.p, 0, (size_t)nshots * c->slot_stride * sizeof(T), c->st));
+    CK(cudaMemsetAsync(c->psi.p, 0, (size_t)nshots * c->psi_slot * sizeof(T), c->st));
+    return IFOS_OK;
+}
+
+template <typename T>
+static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
+    const ifos_params &p = c->p;
+    Launcher<T> Lr(c, nshots);
+    if (int rc = zero_state<T>(c, nshots)) return rc;
+    CK(cudaMemsetAsync(c->sec.p, 0, (size_t)nshots * IFOS_NS * std::max(1, p.max_rec) * p.nt * 4, c->st));
+    CK(cudaMemsetAsync(c->bad.p, 0, 4, c->st));
+    const bool snaps = store && c->with_snap;
+    const int ntd = p.nt / p.dtinv;
+    if (snaps && p.snap_format != 0)
+        CK(cudaMemsetAsync(c->snap_scale.p, 0, (size_t)nshots * ntd * c->ncomp * 4, c->st));
+    const bool force = (c->psv && !c->ac && any_force_source(c, nshots)) || c->sh ||
+                       (c->ac && any_force_source(c, nshots));
+    KSnap sn = ksnap(c);
+    CK(cudaEventRecord(c->ev0, c->st));
+    int hin = 0;
+    for (int nt = 1; nt <= nsteps; nt++) {
+        const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
+        Lr.v_step(0, snap_now ? 1 : 0);
+        if (force) {
+            k_inject_v_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
+                                                        c->sh);
+            c->launches++;
+        }
+        Lr.s_step();
+        if (c->psv) {
+            k_psource_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.src, nt, c->ac);
+            c->launches++;
+        }
+        if (p.free_surf) Lr.surface();
+        Lr.seismo(nt);
+        if (snap_now) {
+            if (p.snap_format == 0) {
+                k_snap_store<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
+                c->launches++;
+            } else {
+                k_snap_absmax<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
+                k_snap_quant<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
+                c->launches += 2;
+            }
+            hin++;
+        }
+    }
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    int bad = 0;
+    CK(cudaMemcpy(&bad, c->bad.p, 4, cudaMemcpyDeviceToHost));
+    c->snaps_valid = snaps && nsteps == p.nt;
+    c->fwd_nshots = nshots;
+    if (bad) return fail(c, IFOS_ERR_UNSTABLE, "simulation is unstable (NaN at the grid centre)");
+    return IFOS_OK;
+}
+
+template <typename T>
+static int adjoint_t(ifos_ctx *c, int nshots) {
+    const ifos_params &p = c->p;
+    Launcher<T> Lr(c, nshots);
+    if (int rc = zero_state<T>(c, nshots)) return rc;
+    const long long N = (long long)p.nx * p.ny;
+    CK(cudaMemsetAsync(c->gacc.p, 0, (size_t)nshots * 5 * N * 4, c->st));
+    KSnap sn = ksnap(c);
+    KGrad gr{(float *)c->gacc.p, (float *)c->gout.p, N};
+    const int ntd = p.nt / p.dtinv;
+    const int mr = std::max(1, p.max_rec);
+    dim3 gr_rec((mr + 127) / 128, nshots);
+    CK(cudaEventRecord(c->ev0, c->st));
+    int hin_a = 1;
+    for (int nt = 1; nt <= p.nt; nt++) {
+        Lr.v_step(1, 0);
+        if ((c->psv && p.adjoint_type >= 1 && p.adjoint_type <= 3) || c->sh) {
+            k_inject_v_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->psv ? 1 : 0, c->sh && !c->ac);
+            c->launches++;
+        }
+        Lr.s_step();
+        if (p.adjoint_type == 4) {
+            k_psource_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->ac);
+            c->launches++;
+        }
+        if (p.free_surf) Lr.surface();
+        const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
+        if ((fstep - 1) % p.dtinv == 0) {
+            k_correlate<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, Lr.M, sn, gr, ntd - hin_a, c->psv, c->sh, c->ac);
+            c->launches++;
+            hin_a++;
+        }
+    }
+    k_assemble<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.M, gr, c->psv, c->sh, c->ac);
+    c->launches++;
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_forward(ifos_ctx *c, int nshots, int store, float *sections) {
+    if (!c) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    int rc = c->dbl ? forward_t<double>(c, nshots, store, c->p.nt) : forward_t<float>(c, nshots, store, c->p.nt);
+    if (rc == IFOS_OK && sections) rc = ifos_fetch_sections(c, nshots, sections);
+    return rc;
+}
+
+extern "C" int ifos_stage_adjoint(ifos_ctx *c, int nshots, const float *adj) {
+    if (!c) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots || !adj) return fail(c, IFOS_ERR_ARG, "bad adjoint staging");
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    CK(cudaMemcpyAsync(c->adj.p, adj, (size_t)nshots * 3 * std::max(1, c->p.max_rec) * c->p.nt * 4,
+                       cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->adj_staged = true;
+    return IFOS_OK;
+}
+
+extern "C" int ifos_adjoint(ifos_ctx *c, int nshots, const float *adj, float *grads) {
+    if (!c) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    if (!c->snaps_valid || nshots > c->fwd_nshots)
+        return fail(c, IFOS_ERR_STATE, "adjoint needs a preceding forward run that stored snapshots");
+    if (adj) {
+        if (int rc = ifos_stage_adjoint(c, nshots, adj)) return rc;
+    } else if (!c->adj_staged) {
+        return fail(c, IFOS_ERR_STATE, "no adjoint sources staged");
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    int rc = c->dbl ? adjoint_t<double>(c, nshots) : adjoint_t<float>(c, nshots);
+    if (rc == IFOS_OK && grads) rc = ifos_fetch_grads(c, nshots, grads);
+    return rc;
+}
+
+extern "C" int ifos_fetch_sections(ifos_ctx *c, int nshots, float *sections) {
+    if (!c || !sections) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(sections, c->sec.p, (size_t)nshots * IFOS_NS * std::max(1, c->p.max_rec) * c->p.nt * 4,
+                       cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_fetch_grads(ifos_ctx *c, int nshots, float *grads) {
+    if (!c || !grads) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(grads, c->gout.p, (size_t)nshots * IFOS_NG * c->p.nx * c->p.ny * 4, cudaMemcpyDeviceToHost,
+                       c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_grad_sum(ifos_ctx *c, int nshots, float *out) {
+    if (!c || !out) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    const long long N = (long long)c->p.nx * c->p.ny;
+    DevBuf tmp;
+    if (int rc = dev_alloc(c, tmp, (size_t)5 * N * 4)) return rc;
+    k_grad_sum<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>((const float *)c->gout.p, nshots, N, (float *)tmp.p);
+    c->launches++;
+    cudaError_t e = cudaMemcpyAsync(out, tmp.p, (size_t)5 * N * 4, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    dev_free(tmp);
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
+template <typename T>
+__global__ void k_fields_out(KGrid g, KState<T> S, int slot, const int *ids, int nid, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.nx || j > g.ny) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1), n = (long long)g.nx * g.ny;
+    for (int k = 0; k < nid; k++) out[k * n + q] = ids[k] >= 0 ? (float)fieldp(S, slot, ids[k])[c] : 0.0f;
+}
+
+template <typename T>
+static int fetch_fields_t(ifos_ctx *c, int slot, float *fields) {
+    const long long N = (long long)c->p.nx * c->p.ny;
+    DevBuf tmp, ids;
+    if (int rc = dev_alloc(c, tmp, (size_t)IFOS_NF * N * 4)) return rc;
+    if (int rc = dev_alloc(c, ids, IFOS_NF * sizeof(int))) {
+        dev_free(tmp);
+        return rc;
+    }
+    int idh[IFOS_NF];
+    const int map[IFOS_NF] = {P_VX, P_VY, P_SXX, P_SYY, P_SXY, P_VXP1, P_VYP1, P_VZ, P_SXZ, P_SYZ, P_VZP1, P_SP};
+    for (int k = 0; k < IFOS_NF; k++) idh[k] = c->off[map[k]] >= 0 ? map[k] : -1;
+    cudaMemcpyAsync(ids.p, idh, sizeof idh, cudaMemcpyHostToDevice, c->st);
+    dim3 blk(32, 8), grd((c->p.nx + 31) / 32, (c->p.ny + 7) / 8);
+    k_fields_out<T><<<grd, blk, 0, c->st>>>(c->g, kstate<T>(c), slot, (const int *)ids.p, IFOS_NF, (float *)tmp.p);
+    c->launches++;
+    cudaError_t e = cudaMemcpyAsync(fields, tmp.p, (size_t)IFOS_NF * N * 4, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    dev_free(tmp);
+    dev_free(ids);
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_fetch_fields(ifos_ctx *c, int slot, float *fields) {
+    if (!c || !fields) return IFOS_ERR_ARG;
+    if (slot < 0 || slot >= c->p.max_shots) return fail(c, IFOS_ERR_ARG, "slot out of range");
+    CK(cudaSetDevice(c->device));
+    return c->dbl ? fetch_fields_t<double>(c, slot, fields) : fetch_fields_t<float>(c, slot, fields);
+}
+
+extern "C" int ifos_forward_steps(ifos_ctx *c, int nsteps, float *fields) {
+    if (!c) return IFOS_ERR_ARG;
+    if (nsteps < 1 || nsteps > c->p.nt) return fail(c, IFOS_ERR_ARG, "nsteps out of range");
+    CK(cudaSetDevice(c->device));
+    int rc = c->dbl ? forward_t<double>(c, 1, 0, nsteps) : forward_t<float>(c, 1, 0, nsteps);
+    if (rc == IFOS_OK && fields) rc = ifos_fetch_fields(c, 0, fields);
+    return rc;
+}
+
+extern "C" int ifos_dot_f64(ifos_ctx *c, const float *a, const float *b, size_t n, int device_ptrs, double *out) {
+    if (!c || !a || !out) return IFOS_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    const float *da = a, *db = b;
+    DevBuf ta, tb;
+    if (!device_ptrs) {
+        if (int rc = dev_alloc(c, ta, n * 4 + 4)) return rc;
+        CK(cudaMemcpyAsync(ta.p, a, n * 4, cudaMemcpyHostToDevice, c->st));
+        da = (const float *)ta.p;
+        if (b) {
+            if (int rc = dev_alloc(c, tb, n * 4 + 4)) {
+                dev_free(ta);
+                return rc;
+            }
+            CK(cudaMemcpyAsync(tb.p, b, n * 4, cudaMemcpyHostToDevice, c->st));
+            db = (const float *)tb.p;
+        }
+    }
+    const int nb = 592;  // 4 blocks per SM on 148 SMs; <= 1024 partials
+    k_dot_partial<<<nb, 256, 0, c->st>>>(da, db, (long long)n, (double *)c->dot_partial.p);
+    k_dot_final<<<1, 256, 0, c->st>>>((const double *)c->dot_partial.p, nb, (double *)c->dot_out.p);
+    c->launches += 2;
+    cudaError_t e = cudaMemcpyAsync(out, c->dot_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    dev_free(ta);
+    dev_free(tb);
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_calc_res(ifos_ctx *c, int ntr, const float *obs, const float *syn, float *diff, double *l2,
+                             double *energy) {
+    if (!c || !obs || !syn || ntr < 1) return IFOS_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    const int ns = c->p.nt;
+    const size_t bytes = (size_t)ntr * ns * 4;
+    DevBuf d_obs, d_syn, d_diff, d_tr;
+    int rc = dev_alloc(c, d_obs, bytes);
+    if (!rc) rc = dev_alloc(c, d_syn, bytes);
+    if (!rc) rc = dev_alloc(c, d_diff, bytes);
+    if (!rc) rc = dev_alloc(c, d_tr, (size_t)2 * ntr * sizeof(double));
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        cudaMemcpyAsync(d_obs.p, obs, bytes, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(d_syn.p, syn, bytes, cudaMemcpyHostToDevice, c->st);
+        double *tr = (double *)d_tr.p;
+        k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>((const float *)d_obs.p, (const float *)d_syn.p,
+                                                         (float *)d_diff.p, ntr, ns, c->p.dt, tr, tr + ntr);
+        c->launches++;
+        std::vector<double> h((size_t)2 * ntr);
+        if (diff) cudaMemcpyAsync(diff, d_diff.p, bytes, cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(h.data(), tr, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+        e = cudaStreamSynchronize(c->st);
+        double a = 0, b = 0;
+        for (int k = 0; k < ntr; k++) {
+            a += h[k];
+            b += h[ntr + k];
+        }
+        if (l2) *l2 = a;
+        if (energy) *energy = b;
+    }
+    dev_free(d_obs);
+    dev_free(d_syn);
+    dev_free(d_diff);
+    dev_free(d_tr);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
+extern "C" double ifos_last_ms(const ifos_ctx *c) { return c ? c->last_ms : 0.0; }
+extern "C" long long ifos_launch_count(const ifos_ctx *c) { return c ? c->launches : 0; }
+extern "C" int ifos_sync(ifos_ctx *c) {
+    if (!c) return IFOS_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_fd_coeffs(const ifos_params *p, float *hc7) {
+    if (!p || !hc7) return IFOS_ERR_ARG;
+    return fd_coefficients(p->fdorder, p->maxrelerror, hc7) ? IFOS_OK : IFOS_ERR_ARG;
+}
+
+extern "C" int ifos_cpml_profiles(const ifos_params *p, float *out) {
+    if (!p || !out || p->fw < 0) return IFOS_ERR_ARG;
+    CpmlProfiles pr = cpml_profiles(*p);
+    for (int a = 0; a < 12; a++)
+        for (int h = 0; h <= 2 * p->fw; h++) out[(size_t)a * (2 * p->fw + 1) + h] = pr.arr[a][h];
+    return IFOS_OK;
+}

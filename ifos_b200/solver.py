@@ -1,0 +1,180 @@
+"""Host-side mirror of the reference's shot loop over the C ABI.
+
+``ShotSolver`` keeps the roles of the reference driver's per-shot work
+(src/IFOS2D.c:1076-2724): set the model up once, then per shot run the
+forward time loop (update_v_PML, update_s_*_PML, psource, surface_*_PML,
+seismo_ssg, snapshot store), the adjoint time loop with the zero-lag
+correlation, and the per-shot gradient assembly -- all on the device through
+``libifos_b200.so``.  Inputs and outputs are host numpy arrays laid out as
+``include/ifos_gpu.h`` describes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import IfosError, IfosParams, NF, NG, NS, SNAP_FORMATS
+from .params import ShotParams
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def make_params(p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=1, precision="fp32",
+                snap_format="fp32", hi_order_corrected=False) -> IfosParams:
+    c = IfosParams()
+    _lib.load().ifos_params_default(C.byref(c))
+    for name in ("nx", "ny", "nt", "dh", "dt", "fdorder", "maxrelerror", "fw", "free_surf", "boundary", "vppml",
+                 "fpml", "npower", "k_max_pml", "L", "f_ref", "tau", "wavetype", "acoustic", "parameterization",
+                 "velocity", "seismo", "source_type", "adjoint_type", "dtinv"):
+        setattr(c, name, getattr(p, name))
+    fl = list(p.fl)[:_lib.MAX_L]
+    c.fl = (C.c_float * _lib.MAX_L)(*(fl + [0.0] * (_lib.MAX_L - len(fl))))
+    c.hi_order_corrected = 1 if hi_order_corrected else 0
+    c.precision = {"fp32": 0, "fp64": 1}[precision]
+    c.snap_format = SNAP_FORMATS[snap_format]
+    c.max_shots, c.max_models = int(max_shots), int(max_models)
+    c.max_src, c.max_rec = int(max_src), int(max_rec)
+    return c
+
+
+class ShotSolver:
+    """One device context: ``max_shots`` shot slots stepped together."""
+
+    def __init__(self, p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=1, snapshots=True,
+                 precision="fp32", snap_format="fp32", hi_order_corrected=False, device=0):
+        self.p = p
+        self.lib = _lib.load()
+        self.params = make_params(p, max_shots=max_shots, max_models=max_models, max_src=max_src, max_rec=max_rec,
+                                  precision=precision, snap_format=snap_format,
+                                  hi_order_corrected=hi_order_corrected)
+        self.max_shots, self.max_rec, self.max_src = int(max_shots), int(max_rec), int(max_src)
+        self._ctx = C.c_void_p()
+        rc = self.lib.ifos_ctx_create(C.byref(self.params), int(device), 1 if snapshots else 0, C.byref(self._ctx))
+        if rc != 0:
+            raise IfosError(rc, self.lib.ifos_last_error(None).decode())
+
+    @staticmethod
+    def bytes_needed(p: ShotParams, snapshots=True, **kw) -> int:
+        return int(_lib.load().ifos_ctx_bytes(C.byref(make_params(p, **kw)), 1 if snapshots else 0))
+
+    # -- error handling -------------------------------------------------------
+    def _check(self, rc):
+        if rc != 0:
+            raise IfosError(rc, self.lib.ifos_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self.lib.ifos_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- set-up ---------------------------------------------------------------
+    def upload_model(self, model: dict, index: int = 0):
+        vp, vs, rho = _f32(model["vp"]), _f32(model.get("vs")), _f32(model["rho"])
+        taup, taus = _f32(model.get("taup")), _f32(model.get("taus"))
+        if vs is None:
+            vs = np.zeros_like(vp)
+        self._check(self.lib.ifos_model_upload(self._ctx, int(index), _fp(vp), _fp(vs), _fp(rho), _fp(taup),
+                                               _fp(taus)))
+
+    def setup_shot(self, slot: int, srcpos, signals, recpos, model: int = 0):
+        srcpos = _f32(srcpos)
+        signals = _f32(signals)
+        recpos = np.ascontiguousarray(recpos, dtype=np.int32)
+        nsrc = 0 if srcpos is None else srcpos.shape[1]
+        ntr = recpos.shape[1]
+        self._check(self.lib.ifos_shot_setup(self._ctx, int(slot), int(model), nsrc, _fp(srcpos), _fp(signals), ntr,
+                                             recpos.ctypes.data_as(C.POINTER(C.c_int))))
+
+    # -- time loops -------------------------------------------------------------
+    def forward(self, nshots: int = 1, store: bool = True, fetch: bool = True):
+        """Forward time loop of slots [0, nshots).  Returns sections
+        (nshots, 6, max_rec, NT) when ``fetch``."""
+        out = np.zeros((nshots, NS, self.max_rec, self.p.nt), np.float32) if fetch else None
+        self._check(self.lib.ifos_forward(self._ctx, int(nshots), 1 if store else 0, _fp(out)))
+        return out
+
+    def stage_adjoint(self, adj, nshots: int = 1):
+        adj = _f32(adj)
+        self._check(self.lib.ifos_stage_adjoint(self._ctx, int(nshots), _fp(adj)))
+
+    def adjoint(self, adj=None, nshots: int = 1, fetch: bool = True):
+        """Adjoint time loop + correlation + assembly.  ``adj`` is
+        (nshots, 3, max_rec, NT) time-reversed adjoint sources (None: staged).
+        Returns gradients (nshots, 10, NY, NX) when ``fetch``."""
+        adj = _f32(adj)
+        out = np.zeros((nshots, NG, self.p.ny, self.p.nx), np.float32) if fetch else None
+        self._check(self.lib.ifos_adjoint(self._ctx, int(nshots), _fp(adj), _fp(out)))
+        return out
+
+    def fetch_sections(self, nshots=1):
+        out = np.zeros((nshots, NS, self.max_rec, self.p.nt), np.float32)
+        self._check(self.lib.ifos_fetch_sections(self._ctx, int(nshots), _fp(out)))
+        return out
+
+    def fetch_grads(self, nshots=1):
+        out = np.zeros((nshots, NG, self.p.ny, self.p.nx), np.float32)
+        self._check(self.lib.ifos_fetch_grads(self._ctx, int(nshots), _fp(out)))
+        return out
+
+    def grad_sum(self, nshots=1):
+        out = np.zeros((5, self.p.ny, self.p.nx), np.float32)
+        self._check(self.lib.ifos_grad_sum(self._ctx, int(nshots), _fp(out)))
+        return out
+
+    def forward_steps(self, nsteps: int):
+        out = np.zeros((NF, self.p.ny, self.p.nx), np.float32)
+        self._check(self.lib.ifos_forward_steps(self._ctx, int(nsteps), _fp(out)))
+        return out
+
+    def fields(self, slot=0):
+        out = np.zeros((NF, self.p.ny, self.p.nx), np.float32)
+        self._check(self.lib.ifos_fetch_fields(self._ctx, int(slot), _fp(out)))
+        return out
+
+    # -- reductions -----------------------------------------------------------
+    def dot_f64(self, a, b=None) -> float:
+        a = _f32(a).ravel()
+        b = None if b is None else _f32(b).ravel()
+        out = C.c_double()
+        self._check(self.lib.ifos_dot_f64(self._ctx, a.ctypes.data, None if b is None else b.ctypes.data,
+                                          a.size, 0, C.byref(out)))
+        return out.value
+
+    def calc_res(self, obs, syn):
+        """Residual, misfit and energy of one component (LNORM=2).  Returns
+        (diff time-reversed, L2, energy) with the sums in FP64."""
+        obs, syn = _f32(obs), _f32(syn)
+        diff = np.zeros_like(obs)
+        l2, en = C.c_double(), C.c_double()
+        self._check(self.lib.ifos_calc_res(self._ctx, obs.shape[0], _fp(obs), _fp(syn), _fp(diff), C.byref(l2),
+                                           C.byref(en)))
+        return diff, l2.value, en.value
+
+    # -- accounting -----------------------------------------------------------
+    @property
+    def last_ms(self) -> float:
+        return float(self.lib.ifos_last_ms(self._ctx))
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.ifos_launch_count(self._ctx))

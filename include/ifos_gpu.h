@@ -1,0 +1,183 @@
+/*
+ * ifos_gpu.h -- C ABI of the B200 shot solver (libifos_b200.so).
+ *
+ * Replaces the device-side work of the IFOS2D shot loop:
+ *   forward time loop   src/IFOS2D.c:1651-1894  (update_v_PML, update_s_*_PML,
+ *                       psource, surface_*_PML, seismo_ssg, snapshot store)
+ *   adjoint time loop   src/IFOS2D.c:2224-2438  (same kernels with sw=1 and the
+ *                       zero-lag correlation at :2379-2419)
+ *   gradient assembly   src/IFOS2D.c:2471-2611  (PARAMETERIZATION=1)
+ *   model set-up        src/IFOS2D.c:906-943 (matcopy_elastic, av_mue, av_rho,
+ *                       av_tau, prepare_update_s) and :816 (PML_pro)
+ * The reference exposes these as void C functions over float** arrays plus
+ * global scalars (src/fd.h:206-560); its shot loop, snapshot store, correlation
+ * and assembly are inline in main().  This ABI keeps their roles behind plain
+ * pointers and sizes: the caller owns every host buffer, the library owns the
+ * device state, every call returns an int status and never exits.
+ *
+ * Array conventions
+ *   model / gradient planes: NY x NX floats, row-major, x fastest; element
+ *     (j,i) of the reference's 1-based grid at [(j-1)*NX + (i-1)]
+ *   srcpos: 8 x nsrc floats, row r = the reference's srcpos_loc[r+1][*]
+ *     (x, y as 1-based grid indices, 0, tshift, fc, amp, azimuth, type)
+ *   recpos: 2 x ntr ints, grid x row then grid y row (1-based)
+ *   signals: nsrc x NT; sections: IFOS_NS x ntr x NT (vx, vy, vz, p, curl,
+ *     div); adjoint sources: 3 x ntr x NT (vx, vy, vz-or-p), time-reversed as
+ *     calc_res writes them (src/calc_res.c:220-281)
+ * A context holds `max_shots` shot slots stepped together (batching).  One
+ * context must not be used from two host threads at once; distinct contexts
+ * are independent and each owns its own CUDA stream.
+ */
+#ifndef IFOS_GPU_H
+#define IFOS_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFOS_OK 0
+#define IFOS_ERR_ARG 1      /* invalid argument or parameter combination */
+#define IFOS_ERR_CUDA 2     /* CUDA runtime error (message via ifos_last_error) */
+#define IFOS_ERR_NOMEM 3    /* device allocation failed / admission refused */
+#define IFOS_ERR_UNSTABLE 4 /* NaN/Inf found in the wavefield (src/IFOS2D.c:1660-1672) */
+#define IFOS_ERR_STATE 5    /* call out of order (e.g. adjoint without stored snapshots) */
+
+#define IFOS_MAX_L 8
+#define IFOS_NS 6  /* seismogram planes */
+#define IFOS_NG 10 /* gradient planes, see IFOS_G_* */
+#define IFOS_NF 12 /* field planes, see IFOS_F_* */
+
+enum { IFOS_S_VX = 0, IFOS_S_VY, IFOS_S_VZ, IFOS_S_P, IFOS_S_CURL, IFOS_S_DIV };
+enum {
+    IFOS_G_LAM_RAW = 0, /* waveconv_shot before assembly   (src/IFOS2D.c:2390) */
+    IFOS_G_MU_RAW,      /* waveconv_u_shot before assembly (src/IFOS2D.c:2398) */
+    IFOS_G_RHO_RAW,     /* waveconv_rho_shot before assembly (src/IFOS2D.c:2385) */
+    IFOS_G_VP,          /* per-shot vp gradient  (src/IFOS2D.c:2491) */
+    IFOS_G_VS,          /* per-shot vs gradient  (src/IFOS2D.c:2520) */
+    IFOS_G_RHO,         /* per-shot rho gradient (src/IFOS2D.c:2580) */
+    IFOS_G_MU_Z_RAW,    /* SH waveconv_u_shot_z   (src/IFOS2D.c:2412) */
+    IFOS_G_RHO_Z_RAW,   /* SH waveconv_rho_shot_z (src/IFOS2D.c:2410) */
+    IFOS_G_VS_Z,        /* SH vs gradient  (src/IFOS2D.c:2549) */
+    IFOS_G_RHO_Z        /* SH rho gradient (src/IFOS2D.c:2600) */
+};
+enum {
+    IFOS_F_VX = 0, IFOS_F_VY, IFOS_F_SXX, IFOS_F_SYY, IFOS_F_SXY, IFOS_F_VXP1, IFOS_F_VYP1,
+    IFOS_F_VZ, IFOS_F_SXZ, IFOS_F_SYZ, IFOS_F_VZP1, IFOS_F_SP
+};
+
+/* Snapshot storage formats (the forward wavefield kept for the adjoint). */
+#define IFOS_SNAP_F32 0
+#define IFOS_SNAP_BF16 1 /* bf16 with one fp32 scale per snapshot and component */
+#define IFOS_SNAP_F16 2  /* fp16 with one fp32 scale per snapshot and component */
+
+/* Parameters: the reference's global scalars of the propagation path
+ * (src/globvar.h; read by src/update_v_PML.c:41-48, src/PML_pro.c:88-98,
+ * src/prepare_update_s.c:24-26, src/seismo_ssg.c:30-32) plus the
+ * device-side choices of this library. */
+typedef struct ifos_params {
+    int nx, ny, nt;
+    float dh, dt;
+    int fdorder, maxrelerror;
+    int fw, free_surf, boundary;
+    float vppml, fpml, npower, k_max_pml;
+    int L;
+    float f_ref, tau;
+    float fl[IFOS_MAX_L];
+    int wavetype;         /* 1 P-SV, 2 SH, 3 both */
+    int acoustic;         /* 1: pressure formulation (WAVETYPE 1 only) */
+    int parameterization; /* must be 1 (vp, vs, rho) */
+    int velocity;         /* must be 0 */
+    int seismo;           /* 0..5 as SEISMO */
+    int source_type;      /* default forward source type */
+    int adjoint_type;     /* 1 vx+vy, 2 vy, 3 vx, 4 p */
+    int dtinv;            /* snapshot interval; NT % DTINV == 0 */
+    /* --- device-side choices --- */
+    int hi_order_corrected; /* 1: FDORDER 10/12 P-SV/acoustic use the CPML form of
+                               orders 2-8; 0: the reference's 10/12 branches */
+    int precision;          /* 0: fp32 arithmetic, 1: fp64 (the error oracle) */
+    int snap_format;        /* IFOS_SNAP_* */
+    int max_shots;          /* shot slots stepped together, >= 1 */
+    int max_models;         /* model slots, >= 1 */
+    int max_src, max_rec;   /* per-shot source / receiver capacity */
+} ifos_params;
+
+typedef struct ifos_ctx ifos_ctx;
+
+/* Fill `p` with the defaults of the reference's JSON reader. */
+void ifos_params_default(ifos_params *p);
+
+/* Create a context on CUDA device `device`; allocates all device state,
+ * including max_shots snapshot buffers when `with_snapshots` is non-zero.
+ * Replaces the allocations of src/IFOS2D.c:371-645. */
+int ifos_ctx_create(const ifos_params *p, int device, int with_snapshots, ifos_ctx **out);
+int ifos_ctx_destroy(ifos_ctx *ctx);
+/* Last error message of this context (or of the last failed create when ctx is NULL). */
+const char *ifos_last_error(const ifos_ctx *ctx);
+/* Bytes of device memory a context with these parameters needs. */
+size_t ifos_ctx_bytes(const ifos_params *p, int with_snapshots);
+
+/* Upload model `model` (vp, vs, rho; taup/taus may be NULL meaning TAU) and
+ * rebuild its coefficients: ghost ring, rip/rjp, uipjp, viscoelastic
+ * coefficients.  Replaces src/IFOS2D.c:906-943 / :3240-3265. */
+int ifos_model_upload(ifos_ctx *ctx, int model, const float *vp, const float *vs, const float *rho,
+                      const float *taup, const float *taus);
+
+/* Describe shot `slot`: its model, sources (+ signals nsrc x NT) and receivers. */
+int ifos_shot_setup(ifos_ctx *ctx, int slot, int model, int nsrc, const float *srcpos, const float *signals,
+                    int ntr, const int *recpos);
+
+/* Forward time loop for slots [0, nshots): zero state, step NT times.
+ * Stores snapshots when the context has them and store != 0.  Sections of
+ * slot s go to sections + s * IFOS_NS*max_rec*NT (NULL: keep on device). */
+int ifos_forward(ifos_ctx *ctx, int nshots, int store, float *sections);
+
+/* Adjoint time loop for slots [0, nshots) with adjoint sources
+ * adj + s * 3*max_rec*NT (NULL: use the ones staged by ifos_stage_adjoint),
+ * correlation with the stored snapshots, and per-shot gradient assembly.
+ * Gradients of slot s go to grads + s * IFOS_NG*NY*NX (NULL: keep on device). */
+int ifos_adjoint(ifos_ctx *ctx, int nshots, const float *adj, float *grads);
+
+/* Device-resident pieces of the two calls above, for callers that keep
+ * inputs resident: stage adjoint sources, then run and fetch separately. */
+int ifos_stage_adjoint(ifos_ctx *ctx, int nshots, const float *adj);
+int ifos_fetch_sections(ifos_ctx *ctx, int nshots, float *sections);
+int ifos_fetch_grads(ifos_ctx *ctx, int nshots, float *grads);
+/* Sum of the assembled per-shot gradients (vp, vs, rho, vs_z, rho_z) over
+ * slots [0, nshots), as src/IFOS2D.c:2703-2724: out is 5 x NY x NX. */
+int ifos_grad_sum(ifos_ctx *ctx, int nshots, float *out);
+
+/* Run `nsteps` forward steps of slot 0 from zero state without snapshots and
+ * copy the IFOS_NF field planes to `fields` (parity checks of single steps). */
+int ifos_forward_steps(ifos_ctx *ctx, int nsteps, float *fields);
+/* Copy the current IFOS_NF field planes of `slot` to host. */
+int ifos_fetch_fields(ifos_ctx *ctx, int slot, float *fields);
+
+/* FP64 reductions (misfit, energy, dot products) over n floats on the
+ * device: returns sum(a*b) (b NULL: sum(a*a)) accumulated in double. */
+int ifos_dot_f64(ifos_ctx *ctx, const float *a, const float *b, size_t n, int device_ptrs, double *out);
+
+/* Residuals of one component, LNORM=2, VELOCITY=0 (src/calc_res.c:137-281):
+ * integrates both sections, writes the time-reversed residual to diff
+ * (ntr x NT) and the misfit/energy sums in double. */
+int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, float *diff, double *l2,
+                  double *energy);
+
+/* Host-only set-up queries (no device needed): the FD weights hc[0..6]
+ * (src/holbergcoeff.c:37-108) and the CPML profiles as 12 arrays of 2*FW+1
+ * floats, 1-based, in the order K_x a_x b_x K_x_half a_x_half b_x_half K_y a_y
+ * b_y K_y_half a_y_half b_y_half (src/PML_pro.c:83-316). */
+int ifos_fd_coeffs(const ifos_params *p, float *hc7);
+int ifos_cpml_profiles(const ifos_params *p, float *out);
+
+/* Milliseconds of device time of the last ifos_forward / ifos_adjoint call. */
+double ifos_last_ms(const ifos_ctx *ctx);
+/* Kernel launches issued by this context since creation. */
+long long ifos_launch_count(const ifos_ctx *ctx);
+int ifos_sync(ifos_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
