@@ -22,8 +22,9 @@ EXPORTS = [
     "ifos_params_default", "ifos_ctx_create", "ifos_ctx_destroy", "ifos_last_error", "ifos_ctx_bytes",
     "ifos_model_upload", "ifos_shot_setup", "ifos_forward", "ifos_adjoint", "ifos_stage_adjoint",
     "ifos_fetch_sections", "ifos_fetch_grads", "ifos_grad_sum", "ifos_forward_steps", "ifos_fetch_fields",
-    "ifos_dot_f64", "ifos_calc_res", "ifos_fd_coeffs", "ifos_cpml_profiles", "ifos_last_ms",
-    "ifos_launch_count", "ifos_sync",
+    "ifos_dot_f64", "ifos_calc_res", "ifos_fd_coeffs", "ifos_cpml_profiles", "ifos_kernel_timing",
+    "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_last_ms", "ifos_launch_count",
+    "ifos_sync",
 ]
 
 
@@ -88,6 +89,10 @@ def load():
         "ifos_calc_res": (C.c_int, [vp, C.c_int, FP, FP, FP, DP, DP]),
         "ifos_fd_coeffs": (C.c_int, [P, FP]),
         "ifos_cpml_profiles": (C.c_int, [P, FP]),
+        "ifos_kernel_timing": (C.c_int, [vp, C.c_int]),
+        "ifos_kernel_times": (C.c_int, [vp, DP, C.POINTER(C.c_longlong), C.c_int]),
+        "ifos_grad_sum_device": (C.c_int, [vp, C.c_int, vp]),
+        "ifos_set_stream": (C.c_int, [vp, vp]),
         "ifos_last_ms": (C.c_double, [vp]),
         "ifos_launch_count": (C.c_longlong, [vp]),
         "ifos_sync": (C.c_int, [vp]),

@@ -57,7 +57,59 @@ struct ifos_ctx {
     bool adj_staged = false;
     float last_ms = 0.0f;
     long long launches = 0;
+    cudaStream_t own_st = nullptr;  // the context's own stream (st may be a caller's)
+    // sampled per-kernel timing
+    int prof_stride = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, size_t>> ev_pairs;  // (class, index of start event)
+    double kt_ms[4] = {0, 0, 0, 0};
+    long long kt_n[4] = {0, 0, 0, 0};
 };
+
+// Events for the sampled kernel timing come from a pool that grows on demand.
+static cudaEvent_t pool_event(ifos_ctx *c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+struct KTimer {
+    ifos_ctx *c;
+    int cls;
+    size_t idx = 0;
+    bool on;
+    KTimer(ifos_ctx *cc, int k, bool sample) : c(cc), cls(k), on(sample && cc->prof_stride > 0) {
+        if (!on) return;
+        idx = c->ev_used;
+        cudaEvent_t e = pool_event(c);
+        if (!e) {
+            on = false;
+            return;
+        }
+        cudaEventRecord(e, c->st);
+    }
+    ~KTimer() {
+        if (!on) return;
+        cudaEvent_t e = pool_event(c);
+        if (!e) return;
+        cudaEventRecord(e, c->st);
+        c->ev_pairs.push_back({cls, idx});
+    }
+};
+static void collect_kernel_times(ifos_ctx *c) {
+    for (auto &pr : c->ev_pairs) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, c->ev_pool[pr.second], c->ev_pool[pr.second + 1]) == cudaSuccess) {
+            c->kt_ms[pr.first] += ms;
+            c->kt_n[pr.first]++;
+        }
+    }
+    c->ev_pairs.clear();
+    c->ev_used = 0;
+}
 
 // ----------------------------------------------------------------------------
 static int fail(ifos_ctx *c, int code, const std::string &msg) {
@@ -201,9 +253,10 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
                       &c->src_n, &c->rec_pos, &c->rec_n, &c->adj, &c->sec, &c->snap, &c->snap_scale, &c->gacc,
                       &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
     for (DevBuf *b : bufs) dev_free(*b);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->st) cudaStreamDestroy(c->st);
+    if (c->own_st) cudaStreamDestroy(c->own_st);
     delete c;
     return IFOS_OK;
 }
@@ -237,9 +290,10 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
         return rc;
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed"));
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
         return bail(fail(c, IFOS_ERR_CUDA, "stream/event creation failed"));
+    c->st = c->own_st;
 
     Layout L = layout_of(p);
     KGrid &g = c->g;
@@ -697,13 +751,20 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     int hin = 0;
     for (int nt = 1; nt <= nsteps; nt++) {
         const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
-        Lr.v_step(0, snap_now ? 1 : 0);
+        const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
+        {
+            KTimer t(c, 0, sample);
+            Lr.v_step(0, snap_now ? 1 : 0);
+        }
         if (force) {
             k_inject_v_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
                                                         c->sh);
             c->launches++;
         }
-        Lr.s_step();
+        {
+            KTimer t(c, 1, sample);
+            Lr.s_step();
+        }
         if (c->psv) {
             k_psource_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.src, nt, c->ac);
             c->launches++;
@@ -711,6 +772,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         if (p.free_surf) Lr.surface();
         Lr.seismo(nt);
         if (snap_now) {
+            KTimer t(c, 2, sample);
             if (p.snap_format == 0) {
                 k_snap_store<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
                 c->launches++;
@@ -726,6 +788,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));
     CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    collect_kernel_times(c);
     int bad = 0;
     CK(cudaMemcpy(&bad, c->bad.p, 4, cudaMemcpyDeviceToHost));
     c->snaps_valid = snaps && nsteps == p.nt;
@@ -749,12 +812,19 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     CK(cudaEventRecord(c->ev0, c->st));
     int hin_a = 1;
     for (int nt = 1; nt <= p.nt; nt++) {
-        Lr.v_step(1, 0);
+        const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
+        {
+            KTimer t(c, 0, sample);
+            Lr.v_step(1, 0);
+        }
         if ((c->psv && p.adjoint_type >= 1 && p.adjoint_type <= 3) || c->sh) {
             k_inject_v_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->psv ? 1 : 0, c->sh && !c->ac);
             c->launches++;
         }
-        Lr.s_step();
+        {
+            KTimer t(c, 1, sample);
+            Lr.s_step();
+        }
         if (p.adjoint_type == 4) {
             k_psource_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->ac);
             c->launches++;
@@ -762,6 +832,7 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
         if (p.free_surf) Lr.surface();
         const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
         if ((fstep - 1) % p.dtinv == 0) {
+            KTimer t(c, 3, sample);
             k_correlate<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, Lr.M, sn, gr, ntd - hin_a, c->psv, c->sh, c->ac);
             c->launches++;
             hin_a++;
@@ -773,6 +844,7 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));
     CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    collect_kernel_times(c);
     return IFOS_OK;
 }
 
@@ -986,5 +1058,44 @@ extern "C" int ifos_cpml_profiles(const ifos_params *p, float *out) {
     CpmlProfiles pr = cpml_profiles(*p);
     for (int a = 0; a < 12; a++)
         for (int h = 0; h <= 2 * p->fw; h++) out[(size_t)a * (2 * p->fw + 1) + h] = pr.arr[a][h];
+    return IFOS_OK;
+}
+
+extern "C" int ifos_kernel_timing(ifos_ctx *c, int stride) {
+    if (!c || stride < 0) return IFOS_ERR_ARG;
+    c->prof_stride = stride;
+    return IFOS_OK;
+}
+
+extern "C" int ifos_kernel_times(ifos_ctx *c, double *ms4, long long *count4, int reset) {
+    if (!c) return IFOS_ERR_ARG;
+    for (int k = 0; k < 4; k++) {
+        if (ms4) ms4[k] = c->kt_ms[k];
+        if (count4) count4[k] = c->kt_n[k];
+        if (reset) {
+            c->kt_ms[k] = 0;
+            c->kt_n[k] = 0;
+        }
+    }
+    return IFOS_OK;
+}
+
+extern "C" int ifos_grad_sum_device(ifos_ctx *c, int nshots, float *dev_out) {
+    if (!c || !dev_out) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    const long long N = (long long)c->p.nx * c->p.ny;
+    k_grad_sum<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>((const float *)c->gout.p, nshots, N, dev_out);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_set_stream(ifos_ctx *c, void *stream) {
+    if (!c) return IFOS_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    c->st = stream ? (cudaStream_t)stream : c->own_st;
     return IFOS_OK;
 }

@@ -170,6 +170,27 @@ class ShotSolver:
                                            C.byref(en)))
         return diff, l2.value, en.value
 
+    def grad_sum_device(self, nshots, dev_ptr: int):
+        """Write the summed gradients (5 x NY x NX float32) to device memory."""
+        self._check(self.lib.ifos_grad_sum_device(self._ctx, int(nshots), C.c_void_p(dev_ptr)))
+
+    def set_stream(self, stream_handle):
+        """Launch on the caller's cudaStream_t (an integer handle), or on the
+        context's own stream with None."""
+        self._check(self.lib.ifos_set_stream(self._ctx, None if not stream_handle else C.c_void_p(stream_handle)))
+
+    def kernel_timing(self, stride: int):
+        self._check(self.lib.ifos_kernel_timing(self._ctx, int(stride)))
+
+    def kernel_times(self, reset=True):
+        """(ms, launches) accumulated per kernel class: velocity, stress,
+        snapshot, correlation."""
+        ms = (C.c_double * 4)()
+        n = (C.c_longlong * 4)()
+        self._check(self.lib.ifos_kernel_times(self._ctx, ms, n, 1 if reset else 0))
+        names = ("velocity", "stress", "snapshot", "correlation")
+        return {k: (ms[i], n[i]) for i, k in enumerate(names)}
+
     # -- accounting -----------------------------------------------------------
     @property
     def last_ms(self) -> float:

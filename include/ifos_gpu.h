@@ -171,6 +171,22 @@ int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, fl
 int ifos_fd_coeffs(const ifos_params *p, float *hc7);
 int ifos_cpml_profiles(const ifos_params *p, float *out);
 
+/* Per-kernel timing: every `stride`-th time step (0 = off) the velocity and
+ * stress kernels are bracketed by CUDA events on the context's stream; the
+ * accumulated milliseconds and launch counts of the kernel classes
+ * {velocity, stress, snapshot, correlation} are returned (4 each) and reset. */
+int ifos_kernel_timing(ifos_ctx *ctx, int stride);
+int ifos_kernel_times(ifos_ctx *ctx, double *ms4, long long *count4, int reset);
+
+/* Sum of the assembled gradients written to DEVICE memory (5 x NY x NX
+ * floats at dev_out), for callers that reduce it across GPUs in place. */
+int ifos_grad_sum_device(ifos_ctx *ctx, int nshots, float *dev_out);
+
+/* Launch on the caller's CUDA stream (a cudaStream_t passed as void*), e.g.
+ * to time the library with the caller's events; NULL returns to the
+ * context's own stream.  The caller keeps ownership of its stream. */
+int ifos_set_stream(ifos_ctx *ctx, void *stream);
+
 /* Milliseconds of device time of the last ifos_forward / ifos_adjoint call. */
 double ifos_last_ms(const ifos_ctx *ctx);
 /* Kernel launches issued by this context since creation. */
