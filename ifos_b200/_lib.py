@@ -23,7 +23,7 @@ EXPORTS = [
     "ifos_model_upload", "ifos_shot_setup", "ifos_forward", "ifos_adjoint", "ifos_stage_adjoint",
     "ifos_fetch_sections", "ifos_fetch_grads", "ifos_grad_sum", "ifos_forward_steps", "ifos_fetch_fields",
     "ifos_dot_f64", "ifos_calc_res", "ifos_fd_coeffs", "ifos_cpml_profiles", "ifos_kernel_timing",
-    "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_last_ms", "ifos_launch_count",
+    "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_dot_f64_noalloc", "ifos_last_ms", "ifos_launch_count",
     "ifos_sync",
 ]
 
@@ -93,6 +93,7 @@ def load():
         "ifos_kernel_times": (C.c_int, [vp, DP, C.POINTER(C.c_longlong), C.c_int]),
         "ifos_grad_sum_device": (C.c_int, [vp, C.c_int, vp]),
         "ifos_set_stream": (C.c_int, [vp, vp]),
+        "ifos_dot_f64_noalloc": (C.c_int, [C.c_int, vp, vp, C.c_size_t, vp, DP]),
         "ifos_last_ms": (C.c_double, [vp]),
         "ifos_launch_count": (C.c_longlong, [vp]),
         "ifos_sync": (C.c_int, [vp]),

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifos_b200.so")
-SOURCES = ["ifos_solver.cu", "ifos_setup.cpp"]
+SOURCES = ["ifos_solver.cu", "ifos_setup.cpp", "ifos_noalloc.cu"]
 HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

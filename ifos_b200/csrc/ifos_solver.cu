@@ -241,6 +241,9 @@ extern "C" size_t ifos_ctx_bytes(const ifos_params *p, int with_snapshots) {
     return b;
 }
 
+// error text of context-free entry points, read back by ifos_last_error(NULL)
+void ifos_internal_set_error(const std::string &msg) { g_create_error = msg; }
+
 extern "C" const char *ifos_last_error(const ifos_ctx *ctx) {
     return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }

@@ -187,6 +187,24 @@ int ifos_grad_sum_device(ifos_ctx *ctx, int nshots, float *dev_out);
  * context's own stream.  The caller keeps ownership of its stream. */
 int ifos_set_stream(ifos_ctx *ctx, void *stream);
 
+/* FP64 dot product without any device allocation.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc (code running in
+ * host callbacks or latency-bound loops where an allocation would stall, or
+ * whose device memory is fully budgeted by another framework) and already hold
+ * the data on the device.  Returns sum(a*b) (b NULL: sum(a*a)) over n floats
+ * at DEVICE pointers a, b of `device`, accumulated in double, in *out (host).
+ * Needs no context.  Its scratch is a static array of IFOS_NOALLOC_MAX_BLOCKS+1
+ * doubles that every device loading the library keeps until exit; n is
+ * limited to IFOS_NOALLOC_MAX_N (IFOS_ERR_ARG above it, message in
+ * ifos_last_error(NULL)).  The first call on a device resolves the scratch
+ * address and should come before any stream capture.  Launches go to `stream`
+ * (NULL: the default stream) and the call returns after the result is copied.
+ * All calls on a device share the scratch, so calls that overlap on the GPU
+ * (other host threads, other streams) race. */
+#define IFOS_NOALLOC_MAX_BLOCKS 4096
+#define IFOS_NOALLOC_MAX_N (4096LL * 256 * 32)
+int ifos_dot_f64_noalloc(int device, const float *a, const float *b, size_t n, void *stream, double *out);
+
 /* Milliseconds of device time of the last ifos_forward / ifos_adjoint call. */
 double ifos_last_ms(const ifos_ctx *ctx);
 /* Kernel launches issued by this context since creation. */
