@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifos_b200.so")
 SOURCES = ["ifos_solver.cu", "ifos_setup.cpp", "ifos_noalloc.cu"]
-HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h"]
+HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h", "ifos_tma.cuh", "ifos_tile.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -39,7 +39,17 @@ struct KGrid {
     float eta[9], bip[9], bjm[9], cip[9], cjm[9], bjm_srf[9];
     float taus0, taup0, tausipjp0;  // used when the tau planes are absent
     int adjoint_type;
+    int k_one;       // every CPML K profile value is 1: d/K == d exactly
+    int dh_pow2;     // DH is a power of two: x/DH == x*inv_dh exactly
+    float inv_dh;    // 1/DH (exact when dh_pow2)
 };
+
+// x / DH, exact in both branches: multiplying by the reciprocal of a power of
+// two rounds exactly as the division does.
+template <typename T>
+__device__ __forceinline__ T div_dh(const KGrid &g, T x) {
+    return g.dh_pow2 ? x * (T)g.inv_dh : x / (T)g.dh;
+}
 
 template <typename T>
 struct KState {
@@ -85,10 +95,26 @@ __device__ inline T prof(const KModel<T> &m, const KGrid &g, int which, int h) {
 
 // CPML recursion of every kernel: psi = b*psi + a*d; d = d/K + psi
 template <typename T>
-__device__ inline T cpml(T *psi, T b, T a, T K, T d) {
+__device__ inline T cpml(T *psi, T b, T a, T K, T d, int k_one = 0) {
     T ps = b * *psi + a * d;
     *psi = ps;
-    return d / K + ps;
+    return (k_one ? d : d / K) + ps;
+}
+
+// CPML on precomputed strip indices (0: not in the strip): hx is the 1-based
+// profile index of the x strip (left: i, right: i-NX+2FW), hy that of the y
+// strip (top without free surface: j, bottom: j-NY+2FW).
+__device__ __forceinline__ int strip_x(const KGrid &g, int i) {
+    if (g.boundary || g.fw == 0) return 0;
+    if (i <= g.fw) return i;
+    if (i >= g.nx - g.fw + 1) return i - g.nx + 2 * g.fw;
+    return 0;
+}
+__device__ __forceinline__ int strip_y(const KGrid &g, int j) {
+    if (g.fw == 0) return 0;
+    if (!g.free_surf && j <= g.fw) return j;
+    if (j >= g.ny - g.fw + 1) return j - g.ny + 2 * g.fw;
+    return 0;
 }
 
 // x strips (left: i<=FW, right: i>=NX-FW+1 at h1=i-NX+2FW), src/update_v_PML.c:177-200
@@ -119,6 +145,21 @@ __device__ inline T cpml_y(const KGrid &g, const KModel<T> &M, T *strip, int j, 
                  prof(M, g, kk, h), d);
     }
     return d;
+}
+
+template <typename T>
+__device__ __forceinline__ T cpml_xh(const KGrid &g, const KModel<T> &M, T *strip, int j, int hx, int kk, int ka,
+                                     int kb, T d) {
+    if (!hx) return d;
+    return cpml(strip + (long long)(j - 1) * (2 * g.fw) + (hx - 1), prof(M, g, kb, hx), prof(M, g, ka, hx),
+                prof(M, g, kk, hx), d, g.k_one);
+}
+template <typename T>
+__device__ __forceinline__ T cpml_yh(const KGrid &g, const KModel<T> &M, T *strip, int i, int hy, int kk, int ka,
+                                     int kb, T d) {
+    if (!hy) return d;
+    return cpml(strip + (long long)(hy - 1) * g.nx + (i - 1), prof(M, g, kb, hy), prof(M, g, ka, hy),
+                prof(M, g, kk, hy), d, g.k_one);
 }
 
 // Reads of a stress plane above the free surface.  The reference mirrors

@@ -1,4 +1,6 @@
 // libifos_b200: device context, time loops and the C ABI (include/ifos_gpu.h).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,8 +15,18 @@
 #include "ifos_kernels.cuh"
 #include "ifos_setup.h"
 #include "ifos_snap.cuh"
+#include "ifos_tile.cuh"
 
 using namespace ifos;
+
+// rows of a pipelined tile (32 columns x kTileY rows) and stages of its ring
+static constexpr int kTileY = 16;
+#ifndef IFOS_NST
+#define IFOS_NST 3
+#endif
+static constexpr int kNst = IFOS_NST;
+// largest L on the pipelined path (more SLS fall back to one thread per cell)
+static constexpr int kPipeMaxL = 5;
 
 namespace {
 thread_local std::string g_create_error;
@@ -65,6 +77,11 @@ struct ifos_ctx {
     std::vector<std::pair<int, size_t>> ev_pairs;  // (class, index of start event)
     double kt_ms[4] = {0, 0, 0, 0};
     long long kt_n[4] = {0, 0, 0, 0};
+    // pipelined (TMA) stencil path: fp32, L <= kPipeMaxL
+    bool pipe = false;
+    KMaps maps{};
+    KTma ktma{};
+    int num_sms = 148;
 };
 
 // Events for the sampled kernel timing come from a pool that grows on demand.
@@ -264,6 +281,60 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
     return IFOS_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// fp32 planes of `pitch` x `rows` elements, `planes` of them back to back;
+// boxes of box_w x box_h x 1, zero fill outside
+static bool encode_planes(CUtensorMap *m, void *base, long long pitch, long long rows, long long planes, int box_w,
+                          int box_h) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)rows, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)(pitch * rows) * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)box_h, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Plane tables and tensor maps of the pipelined kernels.  Leaves c->pipe
+// false (one thread per cell) for fp64 and for L > kPipeMaxL.
+static void setup_pipeline(ifos_ctx *c, const Layout &L) {
+    c->pipe = false;
+    if (c->dbl || c->p.L > kPipeMaxL) return;
+    KTma &t = c->ktma;
+    t.planes_per_slot = (int)(L.slot_elems / L.plane);
+    for (int k = 0; k < NP_FIELD; k++) t.pid[k] = c->off[k] < 0 ? 0 : (int)(c->off[k] / L.plane);
+    for (int k = 0; k < 5; k++) t.mem_pid[k] = c->mem_off[k] < 0 ? 0 : (int)(c->mem_off[k] / L.plane);
+    t.model_planes = (int)(L.model_elems / L.plane);
+    for (int m = 0; m < NM_PLANE; m++) t.mid[m] = c->moff[m] < 0 ? 0 : (int)(c->moff[m] / L.plane);
+    const int fdoh = c->g.fdoh, xh = ((fdoh + 3) / 4) * 4;
+    const long long st_planes = (long long)t.planes_per_slot * c->p.max_shots;
+    const long long md_planes = (long long)t.model_planes * c->p.max_models;
+    if (!encode_planes(&c->maps.halo, c->state.p, L.pitch, L.rows, st_planes, 32 + 2 * xh, kTileY + 2 * fdoh) ||
+        !encode_planes(&c->maps.plain, c->state.p, L.pitch, L.rows, st_planes, 32, kTileY) ||
+        !encode_planes(&c->maps.model, c->models.p, L.pitch, L.rows, md_planes, 32, kTileY))
+        return;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
+        c->num_sms = sms;
+    c->pipe = true;
+}
+
 extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snapshots, ifos_ctx **out) {
     ifos_ctx *c = nullptr;
     if (!pp || !out) return fail(c, IFOS_ERR_ARG, "null argument");
@@ -430,6 +501,14 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
                 else ((float *)hb.data())[idx] = pr.arr[a][h];
             }
         CK(cudaMemcpyAsync(c->prof.p, hb.data(), hb.size(), cudaMemcpyHostToDevice, c->st));
+        // exact shortcuts of the kernels: d/K with K == 1 everywhere, x/DH with DH a power of two
+        g.k_one = 1;
+        for (int a : {K_X, K_XH, K_Y, K_YH})
+            for (int h = 0; h <= 2 * p.fw; h++)
+                if (pr.arr[a][h] != 1.0) g.k_one = 0;
+        int ex = 0;
+        g.dh_pow2 = std::frexp(p.dh, &ex) == 0.5f ? 1 : 0;
+        g.inv_dh = g.dh_pow2 ? 1.0f / p.dh : 0.0f;
     }
     // model plane table
     for (int m = 0; m < NM_PLANE; m++) {
@@ -455,6 +534,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     c->ntr_h.assign(S, 0);
     c->slot_model_h.assign(S, 0);
     c->srcpos_h.assign((size_t)S * 8 * ms, 0.0f);
+    setup_pipeline(c, L);
     CK(cudaStreamSynchronize(c->st));
     *out = c;
     return IFOS_OK;
@@ -679,8 +759,75 @@ struct Launcher {
         rec = krec(c);
         grd = dim3((c->p.nx + 31) / 32, (c->p.ny + 7) / 8, ns);
     }
+    // one persistent launch of a pipelined stencil op over all tiles of all slots
+    template <int FD, int NH, int NP, typename Op>
+    void pipelined(const Op &op) {
+        using P = Pipe<float, FD, kTileY, NH, NP, kNst>;
+        auto kern = kp_stencil<float, FD, kTileY, NH, NP, kNst, Op>;
+        constexpr int kMaxDev = 64;
+        static int occ[kMaxDev] = {0};  // resident blocks per SM, per device (0: not queried)
+        const int d = c->device < kMaxDev ? c->device : kMaxDev - 1;
+        if (!occ[d]) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::bytes());
+            int o = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kBlockThreads, P::bytes());
+            occ[d] = o > 0 ? o : 1;
+        }
+        const long long ntiles =
+            (long long)((c->p.nx + 31) / 32) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
+        const int grid = (int)std::min<long long>(ntiles, (long long)occ[d] * c->num_sms);
+        kern<<<grid, dim3(32, 9), P::bytes(), c->st>>>(c->maps, op, nshots, (int *)c->bad.p);
+    }
+    template <int FD>
+    void v_pipe(int sw, int want_p1) {
+        const KGrid &g = c->g;
+        const KTma &t = c->ktma;
+        if (c->ac) {
+            if (sw) pipelined<FD, 1, 6>(OpVAc<float, FD, kTileY, 6, kNst>{g, S, M, t, sw, want_p1});
+            else pipelined<FD, 1, 4>(OpVAc<float, FD, kTileY, 4, kNst>{g, S, M, t, sw, want_p1});
+            return;
+        }
+        if (c->psv) {
+            if (sw) pipelined<FD, 3, 6>(OpVPsv<float, FD, kTileY, 6, kNst>{g, S, M, t, sw, want_p1});
+            else pipelined<FD, 3, 4>(OpVPsv<float, FD, kTileY, 4, kNst>{g, S, M, t, sw, want_p1});
+        }
+        if (c->sh) pipelined<FD, 2, 2>(OpVSh<float, FD, kTileY, kNst>{g, S, M, t});
+    }
+    template <int FD, int LL>
+    void s_visc_pipe() {
+        const KGrid &g = c->g;
+        if (c->psv) pipelined<FD, 2, 3 + 3 * LL + 6>(OpSVisc<float, FD, kTileY, LL, kNst>{g, S, M, c->ktma});
+        if (c->sh) pipelined<FD, 1, 2 + 2 * LL + 4>(OpSShVisc<float, FD, kTileY, LL, kNst>{g, S, M, c->ktma});
+    }
+    template <int FD>
+    void s_pipe() {
+        const KGrid &g = c->g;
+        const KTma &t = c->ktma;
+        if (c->ac) {
+            pipelined<FD, 2, 2>(OpPAc<float, FD, kTileY, kNst>{g, S, M, t});
+            return;
+        }
+        switch (g.L) {
+            case 0:
+                if (c->psv) pipelined<FD, 2, 6>(OpSEl<float, FD, kTileY, kNst>{g, S, M, t});
+                if (c->sh) pipelined<FD, 1, 4>(OpSShEl<float, FD, kTileY, kNst>{g, S, M, t});
+                break;
+            case 1: s_visc_pipe<FD, 1>(); break;
+            case 2: s_visc_pipe<FD, 2>(); break;
+            case 3: s_visc_pipe<FD, 3>(); break;
+            case 4: s_visc_pipe<FD, 4>(); break;
+            default: s_visc_pipe<FD, 5>(); break;
+        }
+    }
     void v_step(int sw, int want_p1) {
         const KGrid &g = c->g;
+        if constexpr (std::is_same<T, float>::value) {
+            if (c->pipe) {
+                DISPATCH_FDOH(g.fdoh, v_pipe<FD>(sw, want_p1));
+                c->launches += (c->ac ? 1 : c->psv + c->sh);
+                return;
+            }
+        }
         DISPATCH_FDOH(g.fdoh, {
             if (c->ac) k_v_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M, sw, want_p1);
             else {
@@ -692,6 +839,13 @@ struct Launcher {
     }
     void s_step() {
         const KGrid &g = c->g;
+        if constexpr (std::is_same<T, float>::value) {
+            if (c->pipe) {
+                DISPATCH_FDOH(g.fdoh, s_pipe<FD>());
+                c->launches += (c->ac ? 1 : c->psv + c->sh);
+                return;
+            }
+        }
         DISPATCH_FDOH(g.fdoh, {
             if (c->ac) k_p_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
             else {
@@ -727,6 +881,13 @@ static bool any_force_source(const ifos_ctx *c, int nshots) {
             if (t == 2 || t == 3 || t == 4) return true;
         }
     return false;
+}
+
+// error codes >= 16 in the status word come from a bounded barrier wait of a
+// pipelined kernel that gave up (16/17: a consumer on a stage's loads, 18: the
+// producer on a stage's release)
+static int pipeline_timeout(ifos_ctx *c, int code) {
+    return fail(c, IFOS_ERR_CUDA, "pipelined stencil kernel: barrier wait timed out (code " + std::to_string(code) + ")");
 }
 
 template <typename T>
@@ -796,6 +957,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     CK(cudaMemcpy(&bad, c->bad.p, 4, cudaMemcpyDeviceToHost));
     c->snaps_valid = snaps && nsteps == p.nt;
     c->fwd_nshots = nshots;
+    if (bad >= 16) return pipeline_timeout(c, bad);
     if (bad) return fail(c, IFOS_ERR_UNSTABLE, "simulation is unstable (NaN at the grid centre)");
     return IFOS_OK;
 }
@@ -807,6 +969,7 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     if (int rc = zero_state<T>(c, nshots)) return rc;
     const long long N = (long long)p.nx * p.ny;
     CK(cudaMemsetAsync(c->gacc.p, 0, (size_t)nshots * 5 * N * 4, c->st));
+    CK(cudaMemsetAsync(c->bad.p, 0, 4, c->st));
     KSnap sn = ksnap(c);
     KGrad gr{(float *)c->gacc.p, (float *)c->gout.p, N};
     const int ntd = p.nt / p.dtinv;
@@ -848,6 +1011,9 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     CK(cudaEventSynchronize(c->ev1));
     CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
     collect_kernel_times(c);
+    int bad = 0;
+    CK(cudaMemcpy(&bad, c->bad.p, 4, cudaMemcpyDeviceToHost));
+    if (bad >= 16) return pipeline_timeout(c, bad);
     return IFOS_OK;
 }
 
