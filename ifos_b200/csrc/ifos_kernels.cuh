@@ -93,6 +93,16 @@ __device__ inline T prof(const KModel<T> &m, const KGrid &g, int which, int h) {
     return m.prof[which * (2 * g.fw + 1) + h];
 }
 
+// Running sum of the FD taps: the m=1 term starts the sum, as in the
+// reference's written-out expressions (src/update_v_PML.c:164-175); with z0
+// it is added to zero, as in its generic loops (the FDORDER 10/12 default
+// branches of src/update_v_acoustic_PML.c, src/update_p_PML.c and
+// src/update_s_visc_PML.c).  The two differ only in the sign of a zero sum.
+template <typename T>
+__device__ __forceinline__ T tap(int m, T s, T t, bool z0 = false) {
+    return (m == 1 && !z0) ? t : s + t;
+}
+
 // CPML recursion of every kernel: psi = b*psi + a*d; d = d/K + psi
 template <typename T>
 __device__ inline T cpml(T *psi, T b, T a, T K, T d, int k_one = 0) {
@@ -147,21 +157,6 @@ __device__ inline T cpml_y(const KGrid &g, const KModel<T> &M, T *strip, int j, 
     return d;
 }
 
-template <typename T>
-__device__ __forceinline__ T cpml_xh(const KGrid &g, const KModel<T> &M, T *strip, int j, int hx, int kk, int ka,
-                                     int kb, T d) {
-    if (!hx) return d;
-    return cpml(strip + (long long)(j - 1) * (2 * g.fw) + (hx - 1), prof(M, g, kb, hx), prof(M, g, ka, hx),
-                prof(M, g, kk, hx), d, g.k_one);
-}
-template <typename T>
-__device__ __forceinline__ T cpml_yh(const KGrid &g, const KModel<T> &M, T *strip, int i, int hy, int kk, int ka,
-                                     int kb, T d) {
-    if (!hy) return d;
-    return cpml(strip + (long long)(hy - 1) * g.nx + (i - 1), prof(M, g, kb, hy), prof(M, g, ka, hy),
-                prof(M, g, kk, hy), d, g.k_one);
-}
-
 // Reads of a stress plane above the free surface.  The reference mirrors
 // syy, sxy (and syz, sp) into the ghost rows after every stress update
 // (src/surface_elastic_PML.c:53-63: syy[1-m] = -syy[1+m], sxy[1-m] = -sxy[m]);
@@ -195,13 +190,13 @@ __global__ void k_v_psv(KGrid g, KState<T> S, KModel<T> M, int sw, int want_p1) 
         const T dtdh = DT * DT / DH;
         T ax = 0, ay = 0;
 #pragma unroll
-        for (int m = 1; m <= FDOH; m++) ax += (T)g.hc[m] * (sxx[pidx(g, j, i + m)] - sxx[pidx(g, j, i - m + 1)]);
+        for (int m = 1; m <= FDOH; m++) ax = tap(m, ax, (T)g.hc[m] * (sxx[pidx(g, j, i + m)] - sxx[pidx(g, j, i - m + 1)]));
 #pragma unroll
         for (int m = 1; m <= FDOH; m++)
             ax += (T)g.hc[m] * (ld_mirror_odd(g, sxy, j + m - 1, i) - ld_mirror_odd(g, sxy, j - m, i));
 #pragma unroll
         for (int m = 1; m <= FDOH; m++)
-            ay += (T)g.hc[m] * (ld_mirror_even(g, syy, j + m, i) - ld_mirror_even(g, syy, j - m + 1, i));
+            ay = tap(m, ay, (T)g.hc[m] * (ld_mirror_even(g, syy, j + m, i) - ld_mirror_even(g, syy, j - m + 1, i)));
 #pragma unroll
         for (int m = 1; m <= FDOH; m++) ay += (T)g.hc[m] * (sxy[pidx(g, j, i + m - 1)] - sxy[pidx(g, j, i - m)]);
         vx[c] += ax * dtdh * rip;
@@ -210,15 +205,15 @@ __global__ void k_v_psv(KGrid g, KState<T> S, KModel<T> M, int sw, int want_p1) 
     }
     T sxx_x = 0, sxy_x = 0, sxy_y = 0, syy_y = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) sxx_x += (T)g.hc[m] * (sxx[pidx(g, j, i + m)] - sxx[pidx(g, j, i - m + 1)]);
+    for (int m = 1; m <= FDOH; m++) sxx_x = tap(m, sxx_x, (T)g.hc[m] * (sxx[pidx(g, j, i + m)] - sxx[pidx(g, j, i - m + 1)]));
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) sxy_x += (T)g.hc[m] * (sxy[pidx(g, j, i + m - 1)] - sxy[pidx(g, j, i - m)]);
-#pragma unroll
-    for (int m = 1; m <= FDOH; m++)
-        sxy_y += (T)g.hc[m] * (ld_mirror_odd(g, sxy, j + m - 1, i) - ld_mirror_odd(g, sxy, j - m, i));
+    for (int m = 1; m <= FDOH; m++) sxy_x = tap(m, sxy_x, (T)g.hc[m] * (sxy[pidx(g, j, i + m - 1)] - sxy[pidx(g, j, i - m)]));
 #pragma unroll
     for (int m = 1; m <= FDOH; m++)
-        syy_y += (T)g.hc[m] * (ld_mirror_even(g, syy, j + m, i) - ld_mirror_even(g, syy, j - m + 1, i));
+        sxy_y = tap(m, sxy_y, (T)g.hc[m] * (ld_mirror_odd(g, sxy, j + m - 1, i) - ld_mirror_odd(g, sxy, j - m, i)));
+#pragma unroll
+    for (int m = 1; m <= FDOH; m++)
+        syy_y = tap(m, syy_y, (T)g.hc[m] * (ld_mirror_even(g, syy, j + m, i) - ld_mirror_even(g, syy, j - m + 1, i)));
     sxx_x = cpml_x(g, M, S.psix[X_SXX] + slot * S.psix_slot, j, i, K_XH, A_XH, B_XH, sxx_x);
     sxy_x = cpml_x(g, M, S.psix[X_SXY] + slot * S.psix_slot, j, i, K_X, A_X, B_X, sxy_x);
     syy_y = cpml_y(g, M, S.psiy[Y_SYY] + slot * S.psiy_slot, j, i, K_YH, A_YH, B_YH, syy_y);
@@ -251,10 +246,10 @@ __global__ void k_v_sh(KGrid g, KState<T> S, KModel<T> M) {
     const T DT = g.dt, DH = g.dh;
     T sxz_x = 0, syz_y = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) sxz_x += (T)g.hc[m] * (sxz[pidx(g, j, i + m - 1)] - sxz[pidx(g, j, i - m)]);
+    for (int m = 1; m <= FDOH; m++) sxz_x = tap(m, sxz_x, (T)g.hc[m] * (sxz[pidx(g, j, i + m - 1)] - sxz[pidx(g, j, i - m)]));
 #pragma unroll
     for (int m = 1; m <= FDOH; m++)
-        syz_y += (T)g.hc[m] * (ld_mirror_even(g, syz, j + m, i) - ld_mirror_even(g, syz, j - m + 1, i));
+        syz_y = tap(m, syz_y, (T)g.hc[m] * (ld_mirror_even(g, syz, j + m, i) - ld_mirror_even(g, syz, j - m + 1, i)));
     sxz_x = cpml_x(g, M, S.psix[X_SXZ] + slot * S.psix_slot, j, i, K_X, A_X, B_X, sxz_x);
     syz_y = cpml_y(g, M, S.psiy[Y_SYZ] + slot * S.psiy_slot, j, i, K_YH, A_YH, B_YH, syz_y);
     vzp1[c] = vz[c];
@@ -276,10 +271,10 @@ __global__ void k_v_ac(KGrid g, KState<T> S, KModel<T> M, int sw, int want_p1) {
     const T DT = g.dt, DH = g.dh;
     T sp_x = 0, sp_y = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) sp_x += (T)g.hc[m] * (sp[pidx(g, j, i + m)] - sp[pidx(g, j, i - m + 1)]);
+    for (int m = 1; m <= FDOH; m++) sp_x = tap(m, sp_x, (T)g.hc[m] * (sp[pidx(g, j, i + m)] - sp[pidx(g, j, i - m + 1)]), g.quirk_hi != 0);
 #pragma unroll
     for (int m = 1; m <= FDOH; m++)
-        sp_y += (T)g.hc[m] * (ld_mirror_even(g, sp, j + m, i) - ld_mirror_even(g, sp, j - m + 1, i));
+        sp_y = tap(m, sp_y, (T)g.hc[m] * (ld_mirror_even(g, sp, j + m, i) - ld_mirror_even(g, sp, j - m + 1, i)), g.quirk_hi != 0);
     if (g.quirk_hi) {
         const T dtdh = DT * DT / DH;
         vx[c] += sp_x * dtdh * rip;
@@ -318,13 +313,13 @@ __global__ void k_s_psv_el(KGrid g, KState<T> S, KModel<T> M) {
     const T dhi = DT / DH;
     T vxx = 0, vyx = 0, vxy = 0, vyy = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vxx += (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]);
+    for (int m = 1; m <= FDOH; m++) vxx = tap(m, vxx, (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]));
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vyx += (T)g.hc[m] * (vy[pidx(g, j, i + m)] - vy[pidx(g, j, i - m + 1)]);
+    for (int m = 1; m <= FDOH; m++) vyx = tap(m, vyx, (T)g.hc[m] * (vy[pidx(g, j, i + m)] - vy[pidx(g, j, i - m + 1)]));
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vxy += (T)g.hc[m] * (vx[pidx(g, j + m, i)] - vx[pidx(g, j - m + 1, i)]);
+    for (int m = 1; m <= FDOH; m++) vxy = tap(m, vxy, (T)g.hc[m] * (vx[pidx(g, j + m, i)] - vx[pidx(g, j - m + 1, i)]));
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vyy += (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]);
+    for (int m = 1; m <= FDOH; m++) vyy = tap(m, vyy, (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]));
     vxx = vxx * dhi;
     vyx = vyx * dhi;
     vxy = vxy * dhi;
@@ -362,13 +357,13 @@ __global__ void k_s_psv_visc(KGrid g, KState<T> S, KModel<T> M) {
     const T dhi = (T)(1.0 / (double)DH), dthalbe = (T)((double)DT / 2.0);
     T vxx = 0, vyx = 0, vxy = 0, vyy = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vxx += (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]);
+    for (int m = 1; m <= FDOH; m++) vxx = tap(m, vxx, (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]), g.quirk_hi != 0);
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vyx += (T)g.hc[m] * (vy[pidx(g, j, i + m)] - vy[pidx(g, j, i - m + 1)]);
+    for (int m = 1; m <= FDOH; m++) vyx = tap(m, vyx, (T)g.hc[m] * (vy[pidx(g, j, i + m)] - vy[pidx(g, j, i - m + 1)]), g.quirk_hi != 0);
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vxy += (T)g.hc[m] * (vx[pidx(g, j + m, i)] - vx[pidx(g, j - m + 1, i)]);
+    for (int m = 1; m <= FDOH; m++) vxy = tap(m, vxy, (T)g.hc[m] * (vx[pidx(g, j + m, i)] - vx[pidx(g, j - m + 1, i)]), g.quirk_hi != 0);
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vyy += (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]);
+    for (int m = 1; m <= FDOH; m++) vyy = tap(m, vyy, (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]), g.quirk_hi != 0);
     vxx = vxx * dhi;
     vyx = vyx * dhi;
     vxy = vxy * dhi;
@@ -430,9 +425,9 @@ __global__ void k_s_sh(KGrid g, KState<T> S, KModel<T> M) {
     const T dhi = L ? (T)(1.0 / (double)DH) : DT / DH, dthalbe = (T)((double)DT / 2.0);
     T vzx = 0, vzy = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vzx += (T)g.hc[m] * (vz[pidx(g, j, i + m)] - vz[pidx(g, j, i - m + 1)]);
+    for (int m = 1; m <= FDOH; m++) vzx = tap(m, vzx, (T)g.hc[m] * (vz[pidx(g, j, i + m)] - vz[pidx(g, j, i - m + 1)]));
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vzy += (T)g.hc[m] * (vz[pidx(g, j + m - 1, i)] - vz[pidx(g, j - m, i)]);
+    for (int m = 1; m <= FDOH; m++) vzy = tap(m, vzy, (T)g.hc[m] * (vz[pidx(g, j + m - 1, i)] - vz[pidx(g, j - m, i)]));
     vzx = vzx * dhi;
     vzy = vzy * dhi;
     vzx = cpml_x(g, M, S.psix[X_VZX] + slot * S.psix_slot, j, i, K_XH, A_XH, B_XH, vzx);
@@ -484,9 +479,9 @@ __global__ void k_p_ac(KGrid g, KState<T> S, KModel<T> M) {
     const T dhi = DT / DH;
     T vxx = 0, vyy = 0;
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vxx += (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]);
+    for (int m = 1; m <= FDOH; m++) vxx = tap(m, vxx, (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]), g.quirk_hi != 0);
 #pragma unroll
-    for (int m = 1; m <= FDOH; m++) vyy += (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]);
+    for (int m = 1; m <= FDOH; m++) vyy = tap(m, vyy, (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]), g.quirk_hi != 0);
     if (g.quirk_hi) {
         const T gg = modelp(M, slot, M_VP)[c] * DT;
         sp[c] += (gg * (vxx + vyy)) * dhi;
@@ -497,6 +492,21 @@ __global__ void k_p_ac(KGrid g, KState<T> S, KModel<T> M) {
     vxx = cpml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, i, K_X, A_X, B_X, vxx);
     vyy = cpml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, j, i, K_Y, A_Y, B_Y, vyy);
     sp[c] += modelp(M, slot, M_GAC)[c] * (vxx + vyy);
+}
+
+// Cells of a snapshot that the stencil kernels stored and a later kernel of
+// the same step changes (explosive sources, the free surface): base of the
+// snapshot of slot 0 being stored (NULL: nothing to patch), floats between
+// slots, NX*NY, and the component index of every patched field (-1 absent).
+struct KSnapPatch {
+    float *base;
+    long long slot_floats;
+    long long n;
+    int c_sxx, c_syy, c_sp, c_syz;
+};
+__device__ __forceinline__ void snap_patch(const KSnapPatch &pt, int slot, int comp, const KGrid &g, int j, int i,
+                                           float v) {
+    if (pt.base && comp >= 0) pt.base[slot * pt.slot_floats + comp * pt.n + (long long)(j - 1) * g.nx + (i - 1)] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -573,7 +583,7 @@ __global__ void k_inject_v_adj(KGrid g, KState<T> S, KRec rec, int nt, int psv, 
 // explosive source after the stress update (src/psource.c:37-58); one thread
 // per slot walks the sources in order
 template <typename T>
-__global__ void k_psource_fwd(KGrid g, KState<T> S, KSrc src, int nt, int acoustic) {
+__global__ void k_psource_fwd(KGrid g, KState<T> S, KSrc src, int nt, int acoustic, KSnapPatch pt) {
     const int slot = blockIdx.x;
     if (threadIdx.x) return;
     const int n = src.nsrc[slot];
@@ -598,8 +608,12 @@ __global__ void k_psource_fwd(KGrid g, KState<T> S, KSrc src, int nt, int acoust
             T *sxx = fieldp(S, slot, P_SXX), *syy = fieldp(S, slot, P_SYY);
             sxx[c] = (T)((double)sxx[c] + 0.5 * (double)amp);
             syy[c] = (T)((double)syy[c] + 0.5 * (double)amp);
+            snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
+            snap_patch(pt, slot, pt.c_syy, g, j, i, (float)syy[c]);
         } else {
-            fieldp(S, slot, P_SP)[c] += (T)amp;
+            T *sp = fieldp(S, slot, P_SP);
+            sp[c] += (T)amp;
+            snap_patch(pt, slot, pt.c_sp, g, j, i, (float)sp[c]);
         }
     }
 }
@@ -627,7 +641,7 @@ __global__ void k_psource_adj(KGrid g, KState<T> S, KRec rec, int nt, int acoust
 // src/surface_PML.c:61-173, src/surface_acoustic_PML.c:28-38).  The mirrored
 // ghost rows are not stored: the velocity kernels read them via ld_mirror_*.
 template <typename T, int FDOH>
-__global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, int acoustic) {
+__global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, int acoustic, KSnapPatch pt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int slot = blockIdx.y;
     if (i > g.nx) return;
@@ -635,10 +649,15 @@ __global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, in
     const long long c = pidx(g, j, i);
     if (acoustic) {
         fieldp(S, slot, P_SP)[c] = 0;
+        snap_patch(pt, slot, pt.c_sp, g, j, i, 0.0f);
         return;
     }
-    if (sh) fieldp(S, slot, P_SYZ)[c] = 0;
+    if (sh) {
+        fieldp(S, slot, P_SYZ)[c] = 0;
+        snap_patch(pt, slot, pt.c_syz, g, j, i, 0.0f);
+    }
     if (!psv) return;
+    snap_patch(pt, slot, pt.c_syy, g, j, i, 0.0f);
     const T DT = g.dt, DH = g.dh;
     const T dh24 = (T)(1.0 / (double)DH), dthalbe = (T)((double)DT / 2.0);
     const T *vx = fieldp(S, slot, P_VX), *vy = fieldp(S, slot, P_VY);
@@ -660,6 +679,7 @@ __global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, in
     const T fjm = srf[i - 1], gg = srf[g.nx + i - 1];
     if (!L) {
         sxx[c] += -DT * ((gg * gg) / (gg + fjm) * vxx + gg * vyy);
+        snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
         return;
     }
     const T djm = srf[2 * g.nx + i - 1], e = srf[3 * g.nx + i - 1];
@@ -675,6 +695,7 @@ __global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, in
         sump += *pp;
     }
     sxx[c] += (dthalbe * sump);
+    snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
 }
 
 // receivers (src/seismo_ssg.c:26-140) and the instability probe of

@@ -19,12 +19,18 @@
 
 using namespace ifos;
 
-// rows of a pipelined tile (32 columns x kTileY rows) and stages of its ring
-static constexpr int kTileY = 16;
-#ifndef IFOS_NST
-#define IFOS_NST 3
+// rows of a pipelined tile (kTileX = 64 columns x kTileY rows)
+#ifndef IFOS_TILE_Y
+#define IFOS_TILE_Y 8
 #endif
-static constexpr int kNst = IFOS_NST;
+static constexpr int kTileY = IFOS_TILE_Y;
+
+// Stages of an op's shared-memory ring: three when two blocks of three fit
+// in an SM's 227 KB, else two (the ring then still holds two blocks).
+template <int FD, int NH, int NP, int NO>
+constexpr int ring_stages() {
+    return Pipe<FD, kTileY, NH, NP, NO, 1>::bytes() * 6 + 2048 <= 232448 ? 3 : 2;
+}
 // largest L on the pipelined path (more SLS fall back to one thread per cell)
 static constexpr int kPipeMaxL = 5;
 
@@ -79,6 +85,7 @@ struct ifos_ctx {
     long long kt_n[4] = {0, 0, 0, 0};
     // pipelined (TMA) stencil path: fp32, L <= kPipeMaxL
     bool pipe = false;
+    bool fused_snap = false;  // fp32 snapshots written by the stencil kernels
     KMaps maps{};
     KTma ktma{};
     int num_sms = 148;
@@ -315,7 +322,7 @@ static bool encode_planes(CUtensorMap *m, void *base, long long pitch, long long
 // false (one thread per cell) for fp64 and for L > kPipeMaxL.
 static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     c->pipe = false;
-    if (c->dbl || c->p.L > kPipeMaxL) return;
+    if (c->dbl || c->p.L > kPipeMaxL || L.slot_elems >= (1LL << 31)) return;
     KTma &t = c->ktma;
     t.planes_per_slot = (int)(L.slot_elems / L.plane);
     for (int k = 0; k < NP_FIELD; k++) t.pid[k] = c->off[k] < 0 ? 0 : (int)(c->off[k] / L.plane);
@@ -325,10 +332,16 @@ static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     const int fdoh = c->g.fdoh, xh = ((fdoh + 3) / 4) * 4;
     const long long st_planes = (long long)t.planes_per_slot * c->p.max_shots;
     const long long md_planes = (long long)t.model_planes * c->p.max_models;
-    if (!encode_planes(&c->maps.halo, c->state.p, L.pitch, L.rows, st_planes, 32 + 2 * xh, kTileY + 2 * fdoh) ||
-        !encode_planes(&c->maps.plain, c->state.p, L.pitch, L.rows, st_planes, 32, kTileY) ||
-        !encode_planes(&c->maps.model, c->models.p, L.pitch, L.rows, md_planes, 32, kTileY))
+    if (!encode_planes(&c->maps.halo, c->state.p, L.pitch, L.rows, st_planes, kTileX + 2 * xh, kTileY + 2 * fdoh) ||
+        !encode_planes(&c->maps.plain, c->state.p, L.pitch, L.rows, st_planes, kTileX, kTileY) ||
+        !encode_planes(&c->maps.model, c->models.p, L.pitch, L.rows, md_planes, kTileX, kTileY))
         return;
+    // fp32 snapshots are written by the stencil kernels themselves
+    t.snap_ntd = c->p.nt / c->p.dtinv;
+    t.snap_ncomp = c->ncomp;
+    for (int k = 0; k < NP_FIELD; k++) t.snap_comp[k] = -1;
+    for (int k = 0; k < c->ncomp; k++) t.snap_comp[c->comp_plane[k]] = k;
+    c->fused_snap = c->with_snap && c->p.snap_format == 0;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
         c->num_sms = sms;
@@ -760,10 +773,11 @@ struct Launcher {
         grd = dim3((c->p.nx + 31) / 32, (c->p.ny + 7) / 8, ns);
     }
     // one persistent launch of a pipelined stencil op over all tiles of all slots
-    template <int FD, int NH, int NP, typename Op>
+    template <typename Op>
     void pipelined(const Op &op) {
-        using P = Pipe<float, FD, kTileY, NH, NP, kNst>;
-        auto kern = kp_stencil<float, FD, kTileY, NH, NP, kNst, Op>;
+        using P = typename Op::P;
+        static_assert(P::bytes() + 1024 <= 232448, "shared-memory ring exceeds 227 KB");
+        auto kern = kp_stencil<Op>;
         constexpr int kMaxDev = 64;
         static int occ[kMaxDev] = {0};  // resident blocks per SM, per device (0: not queried)
         const int d = c->device < kMaxDev ? c->device : kMaxDev - 1;
@@ -774,56 +788,112 @@ struct Launcher {
             occ[d] = o > 0 ? o : 1;
         }
         const long long ntiles =
-            (long long)((c->p.nx + 31) / 32) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
+            (long long)((c->p.nx + kTileX - 1) / kTileX) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
         const int grid = (int)std::min<long long>(ntiles, (long long)occ[d] * c->num_sms);
-        kern<<<grid, dim3(32, 9), P::bytes(), c->st>>>(c->maps, op, nshots, (int *)c->bad.p);
+        kern<<<grid, dim3(32, kComputeWarps + 1), P::bytes(), c->st>>>(c->maps, op, nshots, (int *)c->bad.p);
     }
-    template <int FD>
-    void v_pipe(int sw, int want_p1) {
+    // the snapshot a launch stores (hin < 0: none)
+    KSnapOut snap_out(int hin) const {
+        KSnapOut so{};
+        if (hin >= 0) {
+            so.base = (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes);
+            so.slot_floats = c->snap_slot_bytes / 4;
+            so.n = (long long)c->p.nx * c->p.ny;
+            so.pairs = (c->p.nx % 2) == 0;
+        }
+        return so;
+    }
+    template <int FD, bool Q, int SW, bool P1>
+    void v_one(int hin) {
         const KGrid &g = c->g;
         const KTma &t = c->ktma;
         if (c->ac) {
-            if (sw) pipelined<FD, 1, 6>(OpVAc<float, FD, kTileY, 6, kNst>{g, S, M, t, sw, want_p1});
-            else pipelined<FD, 1, 4>(OpVAc<float, FD, kTileY, 4, kNst>{g, S, M, t, sw, want_p1});
+            constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
+            pipelined(OpVPsv<FD, kTileY, ring_stages<FD, 1, NP, 0>(), Q, SW, P1, true>{g, S, M, t, snap_out(hin)});
             return;
         }
         if (c->psv) {
-            if (sw) pipelined<FD, 3, 6>(OpVPsv<float, FD, kTileY, 6, kNst>{g, S, M, t, sw, want_p1});
-            else pipelined<FD, 3, 4>(OpVPsv<float, FD, kTileY, 4, kNst>{g, S, M, t, sw, want_p1});
+            constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
+            pipelined(OpVPsv<FD, kTileY, ring_stages<FD, 3, NP, 0>(), Q, SW, P1, false>{g, S, M, t, snap_out(hin)});
         }
-        if (c->sh) pipelined<FD, 2, 2>(OpVSh<float, FD, kTileY, kNst>{g, S, M, t});
+    }
+    // hin: snapshot index stored by this step's kernels (-1 none)
+    template <int FD>
+    void v_pipe(int sw, int want_p1, int hin) {
+        bool done = false;
+        if constexpr (FD >= 5) {
+            if (c->g.quirk_hi) {
+                v_one<FD, true, 0, false>(-1);
+                done = true;
+            }
+        }
+        if (!done) {
+            if (sw) v_one<FD, false, 1, false>(-1);
+            else if (want_p1) v_one<FD, false, 0, true>(hin);
+            else v_one<FD, false, 0, false>(-1);
+        }
+        if (c->sh) pipelined(OpVSh<FD, kTileY, ring_stages<FD, 2, 2, 0>()>{c->g, S, M, c->ktma, snap_out(hin)});
     }
     template <int FD, int LL>
-    void s_visc_pipe() {
+    void s_visc_pipe(int hin) {
         const KGrid &g = c->g;
-        if (c->psv) pipelined<FD, 2, 3 + 3 * LL + 6>(OpSVisc<float, FD, kTileY, LL, kNst>{g, S, M, c->ktma});
-        if (c->sh) pipelined<FD, 1, 2 + 2 * LL + 4>(OpSShVisc<float, FD, kTileY, LL, kNst>{g, S, M, c->ktma});
+        constexpr int NST = ring_stages<FD, 2, 3 + 3 * LL + 6, 0>();
+        if (c->psv) {
+            bool done = false;
+            if constexpr (FD >= 5) {
+                if (g.quirk_hi) {
+                    pipelined(OpSVisc<FD, kTileY, LL, NST, true>{g, S, M, c->ktma, snap_out(hin)});
+                    done = true;
+                }
+            }
+            if (!done) pipelined(OpSVisc<FD, kTileY, LL, NST, false>{g, S, M, c->ktma, snap_out(hin)});
+        }
+        if (c->sh) pipelined(OpSSh<FD, kTileY, LL, ring_stages<FD, 1, 2 + 2 * LL + 4, 0>()>{g, S, M, c->ktma, snap_out(hin)});
     }
     template <int FD>
-    void s_pipe() {
+    void s_pipe(int hin) {
         const KGrid &g = c->g;
         const KTma &t = c->ktma;
+        bool quirk = false;
+        if constexpr (FD >= 5) quirk = g.quirk_hi != 0;
         if (c->ac) {
-            pipelined<FD, 2, 2>(OpPAc<float, FD, kTileY, kNst>{g, S, M, t});
+            constexpr int NST = ring_stages<FD, 2, 2, 0>();
+            if constexpr (FD >= 5) {
+                if (quirk) {
+                    pipelined(OpPAc<FD, kTileY, NST, true>{g, S, M, t, snap_out(hin)});
+                    return;
+                }
+            }
+            pipelined(OpPAc<FD, kTileY, NST, false>{g, S, M, t, snap_out(hin)});
             return;
         }
         switch (g.L) {
             case 0:
-                if (c->psv) pipelined<FD, 2, 6>(OpSEl<float, FD, kTileY, kNst>{g, S, M, t});
-                if (c->sh) pipelined<FD, 1, 4>(OpSShEl<float, FD, kTileY, kNst>{g, S, M, t});
+                if (c->psv) {
+                    constexpr int NST = ring_stages<FD, 2, 6, 0>();
+                    bool done = false;
+                    if constexpr (FD >= 5) {
+                        if (quirk) {
+                            pipelined(OpSEl<FD, kTileY, NST, true>{g, S, M, t, snap_out(hin)});
+                            done = true;
+                        }
+                    }
+                    if (!done) pipelined(OpSEl<FD, kTileY, NST, false>{g, S, M, t, snap_out(hin)});
+                }
+                if (c->sh) pipelined(OpSSh<FD, kTileY, 0, ring_stages<FD, 1, 4, 0>()>{g, S, M, t, snap_out(hin)});
                 break;
-            case 1: s_visc_pipe<FD, 1>(); break;
-            case 2: s_visc_pipe<FD, 2>(); break;
-            case 3: s_visc_pipe<FD, 3>(); break;
-            case 4: s_visc_pipe<FD, 4>(); break;
-            default: s_visc_pipe<FD, 5>(); break;
+            case 1: s_visc_pipe<FD, 1>(hin); break;
+            case 2: s_visc_pipe<FD, 2>(hin); break;
+            case 3: s_visc_pipe<FD, 3>(hin); break;
+            case 4: s_visc_pipe<FD, 4>(hin); break;
+            default: s_visc_pipe<FD, 5>(hin); break;
         }
     }
-    void v_step(int sw, int want_p1) {
+    void v_step(int sw, int want_p1, int hin = -1) {
         const KGrid &g = c->g;
         if constexpr (std::is_same<T, float>::value) {
             if (c->pipe) {
-                DISPATCH_FDOH(g.fdoh, v_pipe<FD>(sw, want_p1));
+                DISPATCH_FDOH(g.fdoh, v_pipe<FD>(sw, want_p1, hin));
                 c->launches += (c->ac ? 1 : c->psv + c->sh);
                 return;
             }
@@ -837,11 +907,11 @@ struct Launcher {
         });
         c->launches += (c->ac ? 1 : c->psv + c->sh);
     }
-    void s_step() {
+    void s_step(int hin = -1) {
         const KGrid &g = c->g;
         if constexpr (std::is_same<T, float>::value) {
             if (c->pipe) {
-                DISPATCH_FDOH(g.fdoh, s_pipe<FD>());
+                DISPATCH_FDOH(g.fdoh, s_pipe<FD>(hin));
                 c->launches += (c->ac ? 1 : c->psv + c->sh);
                 return;
             }
@@ -858,10 +928,10 @@ struct Launcher {
         });
         c->launches += (c->ac ? 1 : c->psv + c->sh);
     }
-    void surface() {
+    void surface(const KSnapPatch &pt) {
         const KGrid &g = c->g;
         dim3 gs((c->p.nx + 127) / 128, nshots);
-        DISPATCH_FDOH(g.fdoh, k_surface<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, c->psv, c->sh, c->ac));
+        DISPATCH_FDOH(g.fdoh, k_surface<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, c->psv, c->sh, c->ac, pt));
         c->launches++;
     }
     void seismo(int nt) {
@@ -911,14 +981,31 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     const bool force = (c->psv && !c->ac && any_force_source(c, nshots)) || c->sh ||
                        (c->ac && any_force_source(c, nshots));
     KSnap sn = ksnap(c);
+    // fp32 snapshots stored by the stencil kernels; the source and surface
+    // kernels patch the cells they change afterwards
+    const bool fused = snaps && c->pipe && c->fused_snap;
+    KSnapPatch pt{};
+    pt.slot_floats = c->snap_slot_bytes / 4;
+    pt.n = (long long)p.nx * p.ny;
+    auto comp_of = [&](int plane) {
+        for (int k = 0; k < c->ncomp; k++)
+            if (c->comp_plane[k] == plane) return k;
+        return -1;
+    };
+    pt.c_sxx = comp_of(P_SXX);
+    pt.c_syy = comp_of(P_SYY);
+    pt.c_sp = comp_of(P_SP);
+    pt.c_syz = comp_of(P_SYZ);
     CK(cudaEventRecord(c->ev0, c->st));
     int hin = 0;
     for (int nt = 1; nt <= nsteps; nt++) {
         const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
         const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
+        const int fhin = (fused && snap_now) ? hin : -1;
+        pt.base = fhin >= 0 ? (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes) : nullptr;
         {
             KTimer t(c, 0, sample);
-            Lr.v_step(0, snap_now ? 1 : 0);
+            Lr.v_step(0, snap_now ? 1 : 0, fhin);
         }
         if (force) {
             k_inject_v_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
@@ -927,15 +1014,17 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         }
         {
             KTimer t(c, 1, sample);
-            Lr.s_step();
+            Lr.s_step(fhin);
         }
         if (c->psv) {
-            k_psource_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.src, nt, c->ac);
+            k_psource_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.src, nt, c->ac, pt);
             c->launches++;
         }
-        if (p.free_surf) Lr.surface();
+        if (p.free_surf) Lr.surface(pt);
         Lr.seismo(nt);
-        if (snap_now) {
+        if (snap_now && fused) {
+            hin++;
+        } else if (snap_now) {
             KTimer t(c, 2, sample);
             if (p.snap_format == 0) {
                 k_snap_store<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
@@ -995,7 +1084,7 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
             k_psource_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->ac);
             c->launches++;
         }
-        if (p.free_surf) Lr.surface();
+        if (p.free_surf) Lr.surface(KSnapPatch{});
         const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
         if ((fstep - 1) % p.dtinv == 0) {
             KTimer t(c, 3, sample);

@@ -1,16 +1,24 @@
-// Persistent, TMA-pipelined stencil kernels.
+// Persistent, TMA-pipelined stencil kernels (fp32).
 //
-// Each block loops over 32 x TY tiles of the grid (all shot slots).  A
-// producer warp issues bulk tensor loads (cp.async.bulk.tensor, no multicast)
-// of every input plane of a tile into a ring of NST shared-memory stages: the
-// planes that need neighbours (the stresses in the velocity update, the
-// velocities in the stress update) as tile + halo boxes, and the per-cell
-// streams (the updated fields, memory variables, coefficients) as plain tile
-// boxes.  Eight compute warps consume the stages in order and release each
-// one to the producer, so HBM latency is hidden by the ring rather than by
-// occupancy.  Results are written back with coalesced 128-byte warp stores.
-// The per-cell arithmetic is the reference's, in the same order and with the
-// same float/double promotions as ifos_kernels.cuh.
+// Each block loops over 64 x TY tiles of the grid (all shot slots).  A
+// producer warp streams every input plane of a tile into a ring of NST
+// shared-memory stages with bulk tensor loads (cp.async.bulk.tensor, never
+// with cluster multicast): the planes that need neighbours (the stresses in
+// the velocity update, the velocities in the stress update) as tile + halo
+// boxes, the per-cell planes (fields, memory variables, coefficients) as
+// plain tile boxes.  The compute warps release a stage as soon as they have
+// read it and write their results straight to HBM with 8-byte stores (on
+// snapshot steps also the stored wavefield components, into the snapshot
+// buffer), so the ring only ever waits on loads.
+//
+// A thread owns two adjacent columns (float2 shared-memory accesses) of the
+// RT = TY / (compute warps) consecutive rows of its warp: the x-taps of both
+// columns come from one aligned window, the y-taps of neighbouring rows from
+// the same words, and the cells of a thread are independent work.  Interior
+// tiles (no CPML strip cell) take a path without strip code.  The per-cell
+// arithmetic is the reference's, in the same order and with the same
+// float/double promotions as the one-thread-per-cell kernels of
+// ifos_kernels.cuh.
 #pragma once
 #include <type_traits>
 
@@ -18,58 +26,94 @@
 #include "ifos_tma.cuh"
 
 // 1: the reference's double-promoted terms are evaluated in double (bit-exact);
-// 0: in the kernel's own precision
+// 0: in single precision
 #ifndef IFOS_EXACT
 #define IFOS_EXACT 1
 #endif
 
+// compute warps per block (the block adds one producer warp)
+#ifndef IFOS_NCW
+#define IFOS_NCW 8
+#endif
+
 namespace ifos {
 
-template <typename T>
-using Dbl = typename std::conditional<IFOS_EXACT != 0, double, T>::type;
+constexpr int kComputeWarps = IFOS_NCW;
+constexpr int kBlockThreads = 32 * kComputeWarps + 32;
+constexpr int kTileX = 64;
+
+using D = std::conditional<IFOS_EXACT != 0, double, float>::type;
 
 // Plane ids for the TMA z coordinate: state plane = slot * planes_per_slot + pid,
-// model plane = model * model_planes + mid.
+// model plane = model * model_planes + mid; snap_comp: the snapshot
+// component of a state plane.
 struct KTma {
     int planes_per_slot;
     int pid[NP_FIELD];
     int mem_pid[5];
     int model_planes;
     int mid[NM_PLANE];
-};
-
-template <typename T, int FDOH, int TY, int NH, int NP, int NST>
-struct Pipe {
-    static constexpr int TX = 32, H = FDOH, XH = ((FDOH + 3) / 4) * 4;
-    static constexpr int BW = TX + 2 * XH, BH = TY + 2 * H;
-    static constexpr int ES = (int)sizeof(T);
-    // tensor-copy destinations in shared memory must be 128-byte aligned
-    static constexpr int BOXS = ((BW * BH * ES + 127) / 128) * 128 / ES;
-    static constexpr int PLS = TX * TY;
-    static constexpr int STAGE = NH * BOXS + NP * PLS;
-    static constexpr int RT = TY / 8;  // rows per thread (eight compute warps)
-    static constexpr uint32_t TXB = (uint32_t)((NH * BW * BH + NP * PLS) * ES);
-    static constexpr size_t bytes() { return (size_t)NST * STAGE * ES; }
+    int snap_ntd, snap_ncomp;
+    int snap_comp[NP_FIELD];  // component index of a state plane (-1: not stored)
 };
 
 struct KMaps {
-    CUtensorMap halo;   // state planes, box (32+2XH) x (TY+2H)
-    CUtensorMap plain;  // state planes, box 32 x TY
-    CUtensorMap model;  // model planes, box 32 x TY
+    CUtensorMap halo;   // state planes, box (64+2XH) x (TY+2H)
+    CUtensorMap plain;  // state planes, box 64 x TY (loads and stores)
+    CUtensorMap model;  // model planes, box 64 x TY
 };
 
-struct TileIdx {
-    int slot, i0, j0;
+// fp32 snapshot written by a launch: snapshot of slot 0 being stored (NULL:
+// none), floats between slots, NX*NY, and whether rows start 8-byte aligned
+// (NX even) for pair stores.
+struct KSnapOut {
+    float *base;
+    long long slot_floats, n;
+    int pairs;
 };
-__device__ __forceinline__ TileIdx tile_of(int t, int ntx, int nty, int TY) {
-    TileIdx r;
+
+// NH halo boxes, NP loaded plain boxes, NO output-only plain boxes, NST stages
+template <int FDOH, int TY, int NH, int NP, int NO, int NST>
+struct Pipe {
+    static constexpr int TX = kTileX, H = FDOH;
+    static constexpr int HE = (FDOH + 1) & ~1;       // x window half width (even)
+    static constexpr int XH = ((FDOH + 3) / 4) * 4;  // staged x halo (16-byte TMA alignment)
+    static constexpr int BW = TX + 2 * XH, BH = TY + 2 * H;
+    static constexpr int BOXS = ((BW * BH * 4 + 127) / 128) * 32;  // 128-byte aligned box stride
+    static constexpr int PLS = TX * TY;
+    static constexpr int NHALO = NH, NLOAD = NP, NPL = NP + NO, STAGES = NST;
+    static constexpr int STAGE = NH * BOXS + NPL * PLS;
+    static constexpr int RT = TY / kComputeWarps;  // rows per thread
+    static constexpr int TILE_Y = TY;
+    static constexpr uint32_t TXB = (uint32_t)((NH * BW * BH + NP * PLS) * 4);
+    static constexpr size_t bytes() { return (size_t)NST * STAGE * 4; }
+    static_assert(TY % kComputeWarps == 0, "tile height must be a multiple of the compute warps");
+    static_assert(HE <= XH, "x window exceeds the staged halo");
+};
+
+// One tile as the producer hands it to the compute warps.
+struct __align__(16) TileInfo {
+    int slot, i0, j0;
+    int model;   // model index of the slot
+    int ystrip;  // some row of the tile lies in a CPML y strip
+    int pad[3];
+};
+
+__device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, TileInfo &r) {
     const int per = ntx * nty;
     r.slot = t / per;
     const int rem = t - r.slot * per;
     const int tyi = rem / ntx;
-    r.i0 = (rem - tyi * ntx) * 32 + 1;
+    r.i0 = (rem - tyi * ntx) * kTileX + 1;
     r.j0 = tyi * TY + 1;
-    return r;
+}
+
+// rows j0 .. j0+TY-1 meet a y strip (top: j <= FW without free surface,
+// bottom: j >= NY-FW+1)
+__device__ __forceinline__ int tile_in_ystrip(const KGrid &g, int j0, int TY) {
+    if (g.fw == 0) return 0;
+    if (!g.free_surf && j0 <= g.fw) return 1;
+    return j0 + TY - 1 >= g.ny - g.fw + 1 ? 1 : 0;
 }
 
 // source of a plain-box load: a state plane or a model plane
@@ -78,37 +122,36 @@ struct PlainSrc {
     bool model;
 };
 
-// Warp-specialised persistent driver.  Warps 0-7 compute, warp 8 produces:
-// its lane 0 walks the same tile sequence, waits until a stage has been
-// released by all eight compute warps ("empty" barrier, one arrival per warp),
-// and issues the bulk tensor loads of the next tile into it ("full" barrier,
-// completed by the transaction bytes).  The tile's model index is passed
-// through shared memory.  Every wait is bounded.
-constexpr int kComputeThreads = 256;
-constexpr int kBlockThreads = kComputeThreads + 32;
-
-template <typename T, int FDOH, int TY, int NH, int NP, int NST, typename Op>
-__device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, int nshots, const Op &op,
-                                             const int *slot_model, int *err) {
-    using P = Pipe<T, FDOH, TY, NH, NP, NST>;
+// Warp-specialised persistent driver.  Warps 0..kComputeWarps-1 compute; lane
+// 0 of the last warp produces: it walks the same tile sequence, waits until a
+// stage has been released by all compute warps ("empty" barrier, one arrival
+// per warp), and issues the bulk tensor loads of the next tile into it
+// ("full" barrier, completed by the transaction bytes).  The tile's indices
+// travel through shared memory with the stage.  Every wait is bounded: a
+// wait that gives up records its code in *err (16/17: a compute warp on a
+// stage's loads, 18: the producer on a stage's release) and the block winds
+// down after its copies in flight.
+template <typename P, typename Op>
+__device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, int nshots, const Op &op, int *err) {
+    constexpr int NST = P::STAGES, NH = P::NHALO, NP = P::NLOAD, TY = P::TILE_Y;
     extern __shared__ __align__(1024) unsigned char sm_raw[];
     __shared__ __align__(8) uint64_t full[NST], empty[NST];
-    __shared__ int tile_model[NST];
+    __shared__ TileInfo tinfo[NST];
     __shared__ int abort_flag;
-    T *smem = reinterpret_cast<T *>(sm_raw);
-    const int ntx = (g.nx + 31) / 32, nty = (g.ny + TY - 1) / TY;
+    float *smem = reinterpret_cast<float *>(sm_raw);
+    const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + TY - 1) / TY;
     const int ntiles = ntx * nty * nshots;
-    const int warp = threadIdx.y;  // block is 32 x 9
-    if (warp == 8 && threadIdx.x == 0) {
+    const int warp = threadIdx.y;
+    if (warp == kComputeWarps && threadIdx.x == 0) {
         for (int s = 0; s < NST; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 8);
+            mbar_init(&empty[s], kComputeWarps);
         }
         abort_flag = 0;
         fence_mbar_init();
     }
     __syncthreads();
-    if (warp == 8) {
+    if (warp == kComputeWarps) {
         if (threadIdx.x != 0) return;
         for (int k = 0;; k++) {
             const int t = blockIdx.x + k * gridDim.x;
@@ -118,14 +161,16 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
                 abort_flag = 1;
                 break;
             }
-            const TileIdx ti = tile_of(t, ntx, nty, TY);
-            const int model = slot_model[ti.slot];
-            tile_model[st] = model;
-            T *stage = smem + st * P::STAGE;
+            TileInfo ti;
+            tile_of(t, ntx, nty, TY, ti);
+            ti.model = op.M.slot_model[ti.slot];
+            ti.ystrip = tile_in_ystrip(g, ti.j0, TY);
+            tinfo[st] = ti;
+            float *stage = smem + st * P::STAGE;
             uint64_t *bar = &full[st];
             int hz[NH > 0 ? NH : 1];
             PlainSrc pz[NP > 0 ? NP : 1];
-            op.planes(ti, model, hz, pz);
+            op.planes(ti, hz, pz);
             const int bx = HX + ti.i0 - 1 - P::XH, by = HY + ti.j0 - 1 - P::H;
             const int px = HX + ti.i0 - 1, py = HY + ti.j0 - 1;
             mbar_expect_tx(bar, P::TXB);
@@ -133,8 +178,8 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
             for (int h = 0; h < NH; h++) tma_load_3d(stage + h * P::BOXS, &mp.halo, bx, by, hz[h], bar);
 #pragma unroll
             for (int q = 0; q < NP; q++)
-                tma_load_3d(stage + NH * P::BOXS + q * P::PLS, pz[q].model ? &mp.model : &mp.plain, px, py,
-                            pz[q].z, bar);
+                tma_load_3d(stage + NH * P::BOXS + q * P::PLS, pz[q].model ? &mp.model : &mp.plain, px, py, pz[q].z,
+                            bar);
         }
         return;
     }
@@ -148,375 +193,209 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
             return;
         }
         if (abort_flag) return;
-        const TileIdx ti = tile_of(t, ntx, nty, TY);
-        T *stage = smem + st * P::STAGE;
-        op.compute(ti, tile_model[st], stage, stage + NH * P::BOXS);
-        __syncwarp();
-        if (threadIdx.x == 0) mbar_arrive(&empty[st]);
+        const TileInfo ti = tinfo[st];
+        const float *stage = smem + st * P::STAGE;
+        op.compute(ti, stage, stage + NH * P::BOXS, &empty[st]);
     }
 }
 
-// y-tap of a staged halo tile.  In the top row of tiles with a free surface
-// (MIR) rows j<=0 read the imaged value the reference's ghost rows hold when
-// the velocity is updated: -f(2-j) for syy, syz, sp
-// (src/surface_elastic_PML.c:59) and -f(1-j) for sxy (:60).
-template <bool MIR, bool ODD, typename P, typename T>
-__device__ __forceinline__ T ldy(const T *t, int jj, int col, int dy) {
+// ---------------------------------------------------------------------------
+// Difference stencils of a thread's column pair (cells e = 0, 1 at staged
+// columns c0 + e).  The m=1 term starts each sum and the others are added in
+// order, as in the reference's written-out expressions
+// (src/update_v_PML.c:164-175); Z0: the sum is accumulated from zero, as in
+// its generic loops (the FDORDER 10/12 default branches, e.g.
+// src/update_p_PML.c:275-287).  fwd: sum_m w_m (f[+m] - f[-m+1]);
+// bwd: sum_m w_m (f[+m-1] - f[-m]).
+
+// FD weights of one launch, in registers
+template <int FDOH>
+struct Hc {
+    float w[FDOH + 1];
+    __device__ __forceinline__ explicit Hc(const KGrid &g) {
+#pragma unroll
+        for (int m = 0; m <= FDOH; m++) w[m] = g.hc[m];
+    }
+};
+
+// staged values of one row at columns c0-HE .. c0+HE+1 (c0 - HE even)
+template <int HE>
+struct XWin {
+    float v[2 * HE + 2];
+    __device__ __forceinline__ void load(const float *row, int c0) {
+#pragma unroll
+        for (int q = 0; q <= HE; q++) {
+            const float2 a = *reinterpret_cast<const float2 *>(row + c0 - HE + 2 * q);
+            v[2 * q] = a.x;
+            v[2 * q + 1] = a.y;
+        }
+    }
+};
+template <int FDOH, int HE, bool Z0 = false>
+__device__ __forceinline__ float xfwd(const Hc<FDOH> &hc, const XWin<HE> &W, int e) {
+    float s = hc.w[1] * (W.v[HE + e + 1] - W.v[HE + e]);
+    if (Z0) s = 0.0f + s;
+#pragma unroll
+    for (int m = 2; m <= FDOH; m++) s += hc.w[m] * (W.v[HE + e + m] - W.v[HE + e - m + 1]);
+    return s;
+}
+template <int FDOH, int HE, bool Z0 = false>
+__device__ __forceinline__ float xbwd(const Hc<FDOH> &hc, const XWin<HE> &W, int e) {
+    float s = hc.w[1] * (W.v[HE + e] - W.v[HE + e - 1]);
+    if (Z0) s = 0.0f + s;
+#pragma unroll
+    for (int m = 2; m <= FDOH; m++) s += hc.w[m] * (W.v[HE + e + m - 1] - W.v[HE + e - m]);
+    return s;
+}
+
+// Column pair of a staged halo box at row offset dy from tile row jj.  In the
+// top row of tiles with a free surface (MIR) rows j<=0 read the imaged value
+// the reference's ghost rows hold when the velocity is updated: -f(2-j) for
+// syy, syz, sp (src/surface_elastic_PML.c:59) and -f(1-j) for sxy (:60).
+template <bool MIR, bool ODD, typename P>
+__device__ __forceinline__ float2 ldy2(const float *t, int jj, int c0, int dy) {
     const int rr = jj + P::H + dy;
     if (MIR && rr < P::H) {
         const int src = ODD ? 2 * P::H - rr - 1 : 2 * P::H - rr;
-        return -t[src * P::BW + col];
+        const float2 a = *reinterpret_cast<const float2 *>(t + src * P::BW + c0);
+        return make_float2(-a.x, -a.y);
     }
-    return t[rr * P::BW + col];
+    return *reinterpret_cast<const float2 *>(t + rr * P::BW + c0);
+}
+template <bool MIR, bool ODD, typename P, int FDOH, bool Z0 = false>
+__device__ __forceinline__ float2 yfwd2(const Hc<FDOH> &hc, const float *t, int jj, int c0) {
+    float2 a = ldy2<MIR, ODD, P>(t, jj, c0, 1), b = ldy2<MIR, ODD, P>(t, jj, c0, 0);
+    float2 s = make_float2(hc.w[1] * (a.x - b.x), hc.w[1] * (a.y - b.y));
+    if (Z0) s = make_float2(0.0f + s.x, 0.0f + s.y);
+#pragma unroll
+    for (int m = 2; m <= FDOH; m++) {
+        a = ldy2<MIR, ODD, P>(t, jj, c0, m);
+        b = ldy2<MIR, ODD, P>(t, jj, c0, 1 - m);
+        s.x += hc.w[m] * (a.x - b.x);
+        s.y += hc.w[m] * (a.y - b.y);
+    }
+    return s;
+}
+template <bool MIR, bool ODD, typename P, int FDOH, bool Z0 = false>
+__device__ __forceinline__ float2 ybwd2(const Hc<FDOH> &hc, const float *t, int jj, int c0) {
+    float2 a = ldy2<MIR, ODD, P>(t, jj, c0, 0), b = ldy2<MIR, ODD, P>(t, jj, c0, -1);
+    float2 s = make_float2(hc.w[1] * (a.x - b.x), hc.w[1] * (a.y - b.y));
+    if (Z0) s = make_float2(0.0f + s.x, 0.0f + s.y);
+#pragma unroll
+    for (int m = 2; m <= FDOH; m++) {
+        a = ldy2<MIR, ODD, P>(t, jj, c0, m - 1);
+        b = ldy2<MIR, ODD, P>(t, jj, c0, -m);
+        s.x += hc.w[m] * (a.x - b.x);
+        s.y += hc.w[m] * (a.y - b.y);
+    }
+    return s;
 }
 
-// FD weights of one launch, in registers
-template <typename T, int FDOH>
-struct Hc {
-    T w[FDOH + 1];
-    __device__ __forceinline__ explicit Hc(const KGrid &g) {
-#pragma unroll
-        for (int m = 0; m <= FDOH; m++) w[m] = (T)g.hc[m];
+__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void sts2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+__device__ __forceinline__ float pick(const float2 &v, int e) { return e ? v.y : v.x; }
+
+// CPML on a cell known to lie in the strip (hx / hy > 0), src/update_v_PML.c:177-226
+__device__ __forceinline__ float pml_x(const KGrid &g, const KModel<float> &M, float *strip, int j, int hx, int kk,
+                                       int ka, int kb, float d) {
+    return cpml(strip + (j - 1) * (2 * g.fw) + (hx - 1), prof(M, g, kb, hx), prof(M, g, ka, hx), prof(M, g, kk, hx),
+                d, g.k_one);
+}
+__device__ __forceinline__ float pml_y(const KGrid &g, const KModel<float> &M, float *strip, int i, int hy, int kk,
+                                       int ka, int kb, float d) {
+    return cpml(strip + (hy - 1) * g.nx + (i - 1), prof(M, g, kb, hy), prof(M, g, ka, hy), prof(M, g, kk, hy), d,
+                g.k_one);
+}
+
+// Per-thread geometry of a tile: the column pair, its validity and strip
+// indices, and whether the tile needs the CPML path at all.
+struct Cols {
+    int lane, c0, i;
+    bool v0, v1;
+    int hx0, hx1;
+    __device__ __forceinline__ Cols(const KGrid &g, const TileInfo &ti, int XH, bool strips) {
+        lane = threadIdx.x;
+        c0 = XH + 2 * lane;
+        i = ti.i0 + 2 * lane;
+        v0 = i <= g.nx;
+        v1 = i + 1 <= g.nx;
+        hx0 = (strips && v0) ? strip_x(g, i) : 0;
+        hx1 = (strips && v1) ? strip_x(g, i + 1) : 0;
+    }
+    __device__ __forceinline__ int hx(int e) const { return e ? hx1 : hx0; }
+    __device__ __forceinline__ bool valid(int e) const { return e ? v1 : v0; }
+};
+
+// Store a column pair: both cells (8-byte store) or only the first one
+// (the last column of an odd NX).
+__device__ __forceinline__ void gput2(float *p, float n0, float n1, bool pair, bool v0) {
+    if (pair) *reinterpret_cast<float2 *>(p) = make_float2(n0, n1);
+    else if (v0) *p = n0;
+}
+
+// Row addresses of a thread's column pair: the cell (j, i) in the state of a
+// slot and, on snapshot steps, in the snapshot being stored.
+struct RowOut {
+    float *st;  // state plane 0 at (j, i)
+    float *sn;  // snapshot component 0 at (j, i), NULL when not storing
+    bool pair, v0, spair;
+    __device__ __forceinline__ RowOut(const KGrid &g, const KState<float> &S, const KSnapOut &so, int slot, int j,
+                                      const Cols &cl) {
+        st = S.base + (long long)slot * S.slot_stride + ((j - 1 + HY) * g.pitch + (cl.i - 1 + HX));
+        sn = so.base ? so.base + slot * so.slot_floats + ((long long)(j - 1) * g.nx + (cl.i - 1)) : nullptr;
+        pair = cl.v1;
+        v0 = cl.v0;
+        spair = cl.v1 && so.pairs;
+    }
+    __device__ __forceinline__ void put(long long off, float n0, float n1) const { gput2(st + off, n0, n1, pair, v0); }
+    __device__ __forceinline__ void snap(long long n, int comp, float n0, float n1) const {
+        if (sn && comp >= 0) {
+            float *p = sn + comp * n;
+            if (spair) *reinterpret_cast<float2 *>(p) = make_float2(n0, n1);
+            else {
+                if (v0) p[0] = n0;
+                if (pair) p[1] = n1;
+            }
+        }
     }
 };
+
+// release a stage once every lane of the warp has read its part of it
+__device__ __forceinline__ void release_stage(uint64_t *empty) {
+    __syncwarp();
+    if (threadIdx.x == 0) mbar_arrive(empty);
+}
+
+// Interior tiles take rows<false>; tiles with a strip cell rows<true>.
+#define IFOS_TILE_COMPUTE(NOPML_)                                                                     \
+    __device__ __forceinline__ void compute(const TileInfo &ti, const float *h, const float *pl,      \
+                                            uint64_t *empty) const {                                  \
+        const Cols cl(g, ti, P::XH, !(NOPML_));                                                       \
+        if ((NOPML_) || (cl.hx0 == 0 && cl.hx1 == 0 && !ti.ystrip)) rows<false>(ti, cl, h, pl, empty); \
+        else rows<true>(ti, cl, h, pl, empty);                                                        \
+    }
+
+// the common members of an op
+#define IFOS_OP_MEMBERS \
+    KGrid g;            \
+    KState<float> S;    \
+    KModel<float> M;    \
+    KTma tm;            \
+    KSnapOut so;
 
 // ---------------------------------------------------------------------------
-// velocity, P-SV (src/update_v_PML.c:161-252; 10/12 reference branches :466-528)
-// halo: sxx syy sxy; plain: vx vy rip rjp [+ vxp1 vyp1 in the adjoint, NP=6]
-template <typename T, int FDOH, int TY, int NP, int NST>
-struct OpVPsv {
-    using P = Pipe<T, FDOH, TY, 3, NP, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    int sw, want_p1;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
-        const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
-        hz[0] = zb + tm.pid[P_SXX];
-        hz[1] = zb + tm.pid[P_SYY];
-        hz[2] = zb + tm.pid[P_SXY];
-        pz[0] = {zb + tm.pid[P_VX], false};
-        pz[1] = {zb + tm.pid[P_VY], false};
-        pz[2] = {mb + tm.mid[M_RIP], true};
-        pz[3] = {mb + tm.mid[M_RJP], true};
-        if (NP > 4) {
-            pz[4 % NP] = {zb + tm.pid[P_VXP1], false};
-            pz[5 % NP] = {zb + tm.pid[P_VYP1], false};
-        }
-    }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        if (g.free_surf && ti.j0 == 1) rows<true>(ti, h, pl);
-        else rows<false>(ti, h, pl);
-    }
-    template <bool MIR>
-    __device__ __forceinline__ void rows(const TileIdx &ti, const T *h, const T *pl) const {
-        const T *t_sxx = h, *t_syy = h + P::BOXS, *t_sxy = h + 2 * P::BOXS;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ vx = S.base + so + S.off[P_VX];
-        T *__restrict__ vy = S.base + so + S.off[P_VY];
-        T *__restrict__ vxp1 = S.base + so + S.off[P_VXP1];
-        T *__restrict__ vyp1 = S.base + so + S.off[P_VYP1];
-        T *ps_sxx = S.psix[X_SXX] + slot * S.psix_slot, *ps_sxy = S.psix[X_SXY] + slot * S.psix_slot;
-        T *ps_syy = S.psiy[Y_SYY] + slot * S.psiy_slot, *ps_syx = S.psiy[Y_SXY] + slot * S.psiy_slot;
-        const T DT = g.dt, DH = g.dh;
-        const int col = tx + P::XH;
-#pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
-            if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + col, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            const T vxo = pl[pc], vyo = pl[P::PLS + pc];
-            const T rip = pl[2 * P::PLS + pc], rjp = pl[3 * P::PLS + pc];
-            if (g.quirk_hi) {
-                const T dtdh = DT * DT / DH;
-                T ax = 0, ay = 0;
-#pragma unroll
-                for (int m = 1; m <= FDOH; m++) ax += hc.w[m] * (t_sxx[rc + m] - t_sxx[rc - m + 1]);
-#pragma unroll
-                for (int m = 1; m <= FDOH; m++)
-                    ax += hc.w[m] * (ldy<MIR, true, P>(t_sxy, jj, col, m - 1) - ldy<MIR, true, P>(t_sxy, jj, col, -m));
-#pragma unroll
-                for (int m = 1; m <= FDOH; m++)
-                    ay += hc.w[m] * (ldy<MIR, false, P>(t_syy, jj, col, m) - ldy<MIR, false, P>(t_syy, jj, col, 1 - m));
-#pragma unroll
-                for (int m = 1; m <= FDOH; m++) ay += hc.w[m] * (t_sxy[rc + m - 1] - t_sxy[rc - m]);
-                vx[c] = vxo + ax * dtdh * rip;
-                vy[c] = vyo + ay * dtdh * rjp;
-                continue;
-            }
-            T sxx_x = 0, sxy_x = 0, sxy_y = 0, syy_y = 0;
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) sxx_x += hc.w[m] * (t_sxx[rc + m] - t_sxx[rc - m + 1]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) sxy_x += hc.w[m] * (t_sxy[rc + m - 1] - t_sxy[rc - m]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++)
-                sxy_y += hc.w[m] * (ldy<MIR, true, P>(t_sxy, jj, col, m - 1) - ldy<MIR, true, P>(t_sxy, jj, col, -m));
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++)
-                syy_y += hc.w[m] * (ldy<MIR, false, P>(t_syy, jj, col, m) - ldy<MIR, false, P>(t_syy, jj, col, 1 - m));
-            sxx_x = cpml_xh(g, M, ps_sxx, j, hx, K_XH, A_XH, B_XH, sxx_x);
-            sxy_x = cpml_xh(g, M, ps_sxy, j, hx, K_X, A_X, B_X, sxy_x);
-            syy_y = cpml_yh(g, M, ps_syy, i, hy, K_YH, A_YH, B_YH, syy_y);
-            sxy_y = cpml_yh(g, M, ps_syx, i, hy, K_Y, A_Y, B_Y, sxy_y);
-            if (sw == 0) {
-                if (want_p1) {
-                    vxp1[c] = div_dh(g, rip * (sxx_x + sxy_y));
-                    vyp1[c] = div_dh(g, rjp * (sxy_x + syy_y));
-                }
-            } else if (NP > 4) {
-                vxp1[c] = pl[(4 % NP) * P::PLS + pc] + vxo * DT;
-                vyp1[c] = pl[(5 % NP) * P::PLS + pc] + vyo * DT;
-            }
-            vx[c] = vxo + div_dh(g, DT * rip * (sxx_x + sxy_y));
-            vy[c] = vyo + div_dh(g, DT * rjp * (sxy_x + syy_y));
-        }
-    }
-};
-
-// velocity, SH (src/update_v_PML_SH.c:61-297); halo: sxz syz; plain: vz rjp
-template <typename T, int FDOH, int TY, int NST>
-struct OpVSh {
-    using P = Pipe<T, FDOH, TY, 2, 2, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
-        const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
-        hz[0] = zb + tm.pid[P_SXZ];
-        hz[1] = zb + tm.pid[P_SYZ];
-        pz[0] = {zb + tm.pid[P_VZ], false};
-        pz[1] = {mb + tm.mid[M_RJP], true};
-    }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        if (g.free_surf && ti.j0 == 1) rows<true>(ti, h, pl);
-        else rows<false>(ti, h, pl);
-    }
-    template <bool MIR>
-    __device__ __forceinline__ void rows(const TileIdx &ti, const T *h, const T *pl) const {
-        const T *t_sxz = h, *t_syz = h + P::BOXS;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ vz = S.base + so + S.off[P_VZ];
-        T *__restrict__ vzp1 = S.base + so + S.off[P_VZP1];
-        T *ps_x = S.psix[X_SXZ] + slot * S.psix_slot, *ps_y = S.psiy[Y_SYZ] + slot * S.psiy_slot;
-        const T DT = g.dt;
-        const int col = tx + P::XH;
-#pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
-            if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + col, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            T sxz_x = 0, syz_y = 0;
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) sxz_x += hc.w[m] * (t_sxz[rc + m - 1] - t_sxz[rc - m]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++)
-                syz_y += hc.w[m] * (ldy<MIR, false, P>(t_syz, jj, col, m) - ldy<MIR, false, P>(t_syz, jj, col, 1 - m));
-            sxz_x = cpml_xh(g, M, ps_x, j, hx, K_X, A_X, B_X, sxz_x);
-            syz_y = cpml_yh(g, M, ps_y, i, hy, K_YH, A_YH, B_YH, syz_y);
-            const T vzo = pl[pc];
-            vzp1[c] = vzo;
-            vz[c] = vzo + div_dh(g, pl[P::PLS + pc] * DT * (sxz_x + syz_y));
-        }
-    }
-};
-
-// velocity, acoustic (src/update_v_acoustic_PML.c:72-148, default :396-409)
-// halo: sp; plain: vx vy rip rjp [+ vxp1 vyp1 in the adjoint, NP=6]
-template <typename T, int FDOH, int TY, int NP, int NST>
-struct OpVAc {
-    using P = Pipe<T, FDOH, TY, 1, NP, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    int sw, want_p1;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
-        const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
-        hz[0] = zb + tm.pid[P_SP];
-        pz[0] = {zb + tm.pid[P_VX], false};
-        pz[1] = {zb + tm.pid[P_VY], false};
-        pz[2] = {mb + tm.mid[M_RIP], true};
-        pz[3] = {mb + tm.mid[M_RJP], true};
-        if (NP > 4) {
-            pz[4 % NP] = {zb + tm.pid[P_VXP1], false};
-            pz[5 % NP] = {zb + tm.pid[P_VYP1], false};
-        }
-    }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        if (g.free_surf && ti.j0 == 1) rows<true>(ti, h, pl);
-        else rows<false>(ti, h, pl);
-    }
-    template <bool MIR>
-    __device__ __forceinline__ void rows(const TileIdx &ti, const T *h, const T *pl) const {
-        const T *t_sp = h;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ vx = S.base + so + S.off[P_VX];
-        T *__restrict__ vy = S.base + so + S.off[P_VY];
-        T *__restrict__ vxp1 = S.base + so + S.off[P_VXP1];
-        T *__restrict__ vyp1 = S.base + so + S.off[P_VYP1];
-        T *ps_x = S.psix[X_SXX] + slot * S.psix_slot, *ps_y = S.psiy[Y_SYY] + slot * S.psiy_slot;
-        const T DT = g.dt, DH = g.dh;
-        const int col = tx + P::XH;
-#pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
-            if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + col, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            const T rip = pl[2 * P::PLS + pc], rjp = pl[3 * P::PLS + pc];
-            T sp_x = 0, sp_y = 0;
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) sp_x += hc.w[m] * (t_sp[rc + m] - t_sp[rc - m + 1]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++)
-                sp_y += hc.w[m] * (ldy<MIR, false, P>(t_sp, jj, col, m) - ldy<MIR, false, P>(t_sp, jj, col, 1 - m));
-            const T vxo = pl[pc], vyo = pl[P::PLS + pc];
-            if (g.quirk_hi) {
-                const T dtdh = DT * DT / DH;
-                vx[c] = vxo + sp_x * dtdh * rip;
-                vy[c] = vyo + sp_y * dtdh * rjp;
-                continue;
-            }
-            sp_x = cpml_xh(g, M, ps_x, j, hx, K_XH, A_XH, B_XH, sp_x);
-            sp_y = cpml_yh(g, M, ps_y, i, hy, K_YH, A_YH, B_YH, sp_y);
-            if (sw == 0) {
-                if (want_p1) {
-                    vxp1[c] = div_dh(g, rip * (sp_x));
-                    vyp1[c] = div_dh(g, rjp * (sp_y));
-                }
-            } else if (NP > 4) {
-                vxp1[c] = pl[(4 % NP) * P::PLS + pc] + vxo * DT;
-                vyp1[c] = pl[(5 % NP) * P::PLS + pc] + vyo * DT;
-            }
-            vx[c] = vxo + div_dh(g, DT * rip * (sp_x));
-            vy[c] = vyo + div_dh(g, DT * rjp * (sp_y));
-        }
-    }
-};
-
-// velocity derivatives of the stress kernels from the staged vx, vy tiles
-template <typename P, typename T, int FDOH>
-struct VDer {
-    T vxx, vyx, vxy, vyy;
-    __device__ __forceinline__ VDer(const Hc<T, FDOH> &hc, const T *t_vx, const T *t_vy, int rc) {
-        vxx = 0;
-        vyx = 0;
-        vxy = 0;
-        vyy = 0;
-#pragma unroll
-        for (int m = 1; m <= FDOH; m++) vxx += hc.w[m] * (t_vx[rc + m - 1] - t_vx[rc - m]);
-#pragma unroll
-        for (int m = 1; m <= FDOH; m++) vyx += hc.w[m] * (t_vy[rc + m] - t_vy[rc - m + 1]);
-#pragma unroll
-        for (int m = 1; m <= FDOH; m++) vxy += hc.w[m] * (t_vx[rc + m * P::BW] - t_vx[rc - (m - 1) * P::BW]);
-#pragma unroll
-        for (int m = 1; m <= FDOH; m++) vyy += hc.w[m] * (t_vy[rc + (m - 1) * P::BW] - t_vy[rc - m * P::BW]);
-    }
-};
-
-// stress, P-SV elastic (src/update_s_elastic_PML.c:151-241; 10/12: :442-535)
-// halo: vx vy; plain: sxx syy sxy uipjp f g (reference 10/12 branch: uipjp vs vp)
-template <typename T, int FDOH, int TY, int NST>
-struct OpSEl {
-    using P = Pipe<T, FDOH, TY, 2, 6, NST>;
-    using D = Dbl<T>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
-        const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
-        hz[0] = zb + tm.pid[P_VX];
-        hz[1] = zb + tm.pid[P_VY];
-        pz[0] = {zb + tm.pid[P_SXX], false};
-        pz[1] = {zb + tm.pid[P_SYY], false};
-        pz[2] = {zb + tm.pid[P_SXY], false};
-        pz[3] = {mb + tm.mid[M_UIPJP], true};
-        pz[4] = {mb + tm.mid[g.quirk_hi ? M_VS : M_F], true};
-        pz[5] = {mb + tm.mid[g.quirk_hi ? M_VP : M_G], true};
-    }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        const T *t_vx = h, *t_vy = h + P::BOXS;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ sxx = S.base + so + S.off[P_SXX];
-        T *__restrict__ syy = S.base + so + S.off[P_SYY];
-        T *__restrict__ sxy = S.base + so + S.off[P_SXY];
-        T *ps_vxx = S.psix[X_VXX] + slot * S.psix_slot, *ps_vyx = S.psix[X_VYX] + slot * S.psix_slot;
-        T *ps_vyy = S.psiy[Y_VYY] + slot * S.psiy_slot, *ps_vxy = S.psiy[Y_VXY] + slot * S.psiy_slot;
-        const T DT = g.dt, DH = g.dh;
-        const T dhi = DT / DH;
-#pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
-            if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + tx + P::XH, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            VDer<P, T, FDOH> d(hc, t_vx, t_vy, rc);
-            T vxx = d.vxx * dhi, vyx = d.vyx * dhi, vxy = d.vxy * dhi, vyy = d.vyy * dhi;
-            const T sxx0 = pl[pc], syy0 = pl[P::PLS + pc], sxy0 = pl[2 * P::PLS + pc];
-            if (g.quirk_hi) {
-                const T fipjp = pl[3 * P::PLS + pc] * DT, f = pl[4 * P::PLS + pc] * DT, gg = pl[5 * P::PLS + pc] * DT;
-                sxy[c] = sxy0 + (fipjp * (vxy + vyx));
-                sxx[c] = (T)((D)sxx0 + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vyy)));
-                syy[c] = (T)((D)syy0 + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vxx)));
-                continue;
-            }
-            vxx = cpml_xh(g, M, ps_vxx, j, hx, K_X, A_X, B_X, vxx);
-            vyx = cpml_xh(g, M, ps_vyx, j, hx, K_XH, A_XH, B_XH, vyx);
-            vyy = cpml_yh(g, M, ps_vyy, i, hy, K_Y, A_Y, B_Y, vyy);
-            vxy = cpml_yh(g, M, ps_vxy, i, hy, K_YH, A_YH, B_YH, vxy);
-            const T fipjp = pl[3 * P::PLS + pc], f = pl[4 * P::PLS + pc], gg = pl[5 * P::PLS + pc];
-            sxy[c] = sxy0 + fipjp * (vyx + vxy);
-            sxx[c] = (T)((D)sxx0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vxx)));
-            syy[c] = (T)((D)syy0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vyy)));
-        }
-    }
-};
-
-// stress, P-SV viscoelastic with LL SLS (src/update_s_visc_PML.c)
-// halo: vx vy; plain: sxx syy sxy, r[LL] p[LL] q[LL], fipjp f g mu pi muipjp
-// (non-uniform tau planes are read directly from HBM)
-template <typename T, int FDOH, int TY, int LL, int NST>
+// stress, P-SV viscoelastic with LL SLS (src/update_s_visc_PML.c; the
+// reference 10/12 default :615-660 has no CPML and zero-started sums: QUIRK)
+// halo: vx vy; plain: sxx syy sxy, r[LL] p[LL] q[LL], fipjp f g mu pi muipjp;
+// writes sxx syy sxy r p q.  Non-uniform tau planes are read from HBM.
+template <int FDOH, int TY, int LL, int NST, bool QUIRK>
 struct OpSVisc {
-    static constexpr int NP = 3 + 3 * LL + 6;
-    using P = Pipe<T, FDOH, TY, 2, NP, NST>;
-    using D = Dbl<T>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
+    static constexpr int NH_ = 2, NP_ = 3 + 3 * LL + 6, NOUT = 3 + 3 * LL;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
+        const int mb = ti.model * tm.model_planes;
         hz[0] = zb + tm.pid[P_VX];
         hz[1] = zb + tm.pid[P_VY];
         pz[0] = {zb + tm.pid[P_SXX], false};
@@ -535,284 +414,636 @@ struct OpSVisc {
         pz[3 + 3 * LL + 4] = {mb + tm.mid[M_PIR], true};
         pz[3 + 3 * LL + 5] = {mb + tm.mid[M_MUIPJPR], true};
     }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        const T *t_vx = h, *t_vy = h + P::BOXS;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        const long long mo = (long long)model * M.model_stride;
-        T *__restrict__ sxx = S.base + so + S.off[P_SXX];
-        T *__restrict__ syy = S.base + so + S.off[P_SYY];
-        T *__restrict__ sxy = S.base + so + S.off[P_SXY];
-        T *__restrict__ mr = S.base + so + S.mem_off[0];
-        T *__restrict__ mp = S.base + so + S.mem_off[1];
-        T *__restrict__ mq = S.base + so + S.mem_off[2];
-        T *ps_vxx = S.psix[X_VXX] + slot * S.psix_slot, *ps_vyx = S.psix[X_VYX] + slot * S.psix_slot;
-        T *ps_vyy = S.psiy[Y_VYY] + slot * S.psiy_slot, *ps_vxy = S.psiy[Y_VXY] + slot * S.psiy_slot;
-        const T *ts_p = M.m[M_TAUS] ? M.m[M_TAUS] + mo : nullptr, *tp_p = M.m[M_TAUP] ? M.m[M_TAUP] + mo : nullptr,
-                *tsij_p = M.m[M_TAUSIPJP] ? M.m[M_TAUSIPJP] + mo : nullptr;
-        const long long PL = g.plane;
-        const T DT = g.dt, DH = g.dh;
-        const T dhi = (T)(1.0 / (double)DH), dthalbe = (T)((double)DT / 2.0);
+    IFOS_TILE_COMPUTE(QUIRK)
+    template <bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_vx = h, *t_vy = h + P::BOXS;
+        const Hc<FDOH> hc(g);
+        // everything this warp needs from the stage, then release it
+        XWin<P::HE> wx[RT], wy[RT];
+        float2 dxy[RT], dyy[RT], in[RT][NP_];
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wx[r].load(t_vx + (jj + P::H) * P::BW, cl.c0);
+            wy[r].load(t_vy + (jj + P::H) * P::BW, cl.c0);
+            dxy[r] = yfwd2<false, false, P, FDOH, QUIRK>(hc, t_vx, jj, cl.c0);
+            dyy[r] = ybwd2<false, false, P, FDOH, QUIRK>(hc, t_vy, jj, cl.c0);
+#pragma unroll
+            for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const long long mo = (long long)ti.model * M.model_stride;
+        const float *ts_p = M.m[M_TAUS] ? M.m[M_TAUS] + mo : nullptr;
+        const float *tp_p = M.m[M_TAUP] ? M.m[M_TAUP] + mo : nullptr;
+        const float *tsij_p = M.m[M_TAUSIPJP] ? M.m[M_TAUSIPJP] + mo : nullptr;
+        const float DT = g.dt, DH = g.dh;
+        const float dhi = (float)(1.0 / (double)DH), dthalbe = (float)((double)DT / 2.0);
         constexpr int CO = 3 + 3 * LL;  // first coefficient plane
 #pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
             if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + tx + P::XH, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            VDer<P, T, FDOH> d(hc, t_vx, t_vy, rc);
-            T vxx = d.vxx * dhi, vyx = d.vyx * dhi, vxy = d.vxy * dhi, vyy = d.vyy * dhi;
-            if (!g.quirk_hi) {
-                vxx = cpml_xh(g, M, ps_vxx, j, hx, K_X, A_X, B_X, vxx);
-                vyx = cpml_xh(g, M, ps_vyx, j, hx, K_XH, A_XH, B_XH, vyx);
-                vyy = cpml_yh(g, M, ps_vyy, i, hy, K_Y, A_Y, B_Y, vyy);
-                vxy = cpml_yh(g, M, ps_vxy, i, hy, K_YH, A_YH, B_YH, vxy);
+            float o[NOUT][2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const float2 *v = in[r];
+                float vxx = xbwd<FDOH, P::HE, QUIRK>(hc, wx[r], e) * dhi;
+                float vyx = xfwd<FDOH, P::HE, QUIRK>(hc, wy[r], e) * dhi;
+                float vxy = pick(dxy[r], e) * dhi, vyy = pick(dyy[r], e) * dhi;
+                const bool ok = cl.valid(e);
+                if (PML && ok) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) {
+                        vxx = pml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, vxx);
+                        vyx = pml_x(g, M, S.psix[X_VYX] + slot * S.psix_slot, j, hx, K_XH, A_XH, B_XH, vyx);
+                    }
+                    const int hy = strip_y(g, j);
+                    if (hy) {
+                        vyy = pml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, vyy);
+                        vxy = pml_y(g, M, S.psiy[Y_VXY] + slot * S.psiy_slot, ii, hy, K_YH, A_YH, B_YH, vxy);
+                    }
+                }
+                float sumr = 0, sump = 0, sumq = 0;
+#pragma unroll
+                for (int l = 0; l < LL; l++) {
+                    sumr += pick(v[3 + l], e);
+                    sump += pick(v[3 + LL + l], e);
+                    sumq += pick(v[3 + 2 * LL + l], e);
+                }
+                const float fipjp = pick(v[CO], e), f = pick(v[CO + 1], e), gg = pick(v[CO + 2], e);
+                const float mu = pick(v[CO + 3], e), pi = pick(v[CO + 4], e), muij = pick(v[CO + 5], e);
+                float ts = g.taus0, tp = g.taup0, tsij = g.tausipjp0;
+                if (ok && (ts_p || tp_p || tsij_p)) {
+                    const int c = (j - 1 + HY) * g.pitch + (cl.i + e - 1 + HX);
+                    if (ts_p) ts = ts_p[c];
+                    if (tp_p) tp = tp_p[c];
+                    if (tsij_p) tsij = tsij_p[c];
+                }
+                const float s_xy = pick(v[2], e) + ((fipjp * (vxy + vyx)) + (dthalbe * sumr));
+                const float s_xx = (float)((D)pick(v[0], e) + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vyy) +
+                                                              (D)(dthalbe * sump)));
+                const float s_yy = (float)((D)pick(v[1], e) + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vxx) +
+                                                              (D)(dthalbe * sumq)));
+                sumr = sump = sumq = 0;
+#pragma unroll
+                for (int l = 0; l < LL; l++) {
+                    const float eta = g.eta[l + 1];
+                    // dip, d, e of src/prepare_update_s.c:57-59, formed in the same order
+                    const float dip = muij * eta * tsij, dd = mu * eta * ts, ee = pi * eta * tp;
+                    const float rr = g.bip[l + 1] * (pick(v[3 + l], e) * g.cip[l + 1] - (dip * (vxy + vyx)));
+                    const float pp = (float)((D)g.bjm[l + 1] *
+                                             ((D)(pick(v[3 + LL + l], e) * g.cjm[l + 1] - (ee * (vxx + vyy))) +
+                                              ((D)2 * (D)dd * (D)vyy)));
+                    const float qq = (float)((D)g.bjm[l + 1] *
+                                             ((D)(pick(v[3 + 2 * LL + l], e) * g.cjm[l + 1] - (ee * (vxx + vyy))) +
+                                              ((D)2 * (D)dd * (D)vxx)));
+                    o[3 + l][e] = rr;
+                    o[3 + LL + l][e] = pp;
+                    o[3 + 2 * LL + l][e] = qq;
+                    sumr += rr;
+                    sump += pp;
+                    sumq += qq;
+                }
+                o[0][e] = s_xx + (dthalbe * sump);
+                o[1][e] = s_yy + (dthalbe * sumq);
+                o[2][e] = s_xy + (dthalbe * sumr);
             }
-            T sumr = 0, sump = 0, sumq = 0;
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_SXX], o[0][0], o[0][1]);
+            out.put(S.off[P_SYY], o[1][0], o[1][1]);
+            out.put(S.off[P_SXY], o[2][0], o[2][1]);
 #pragma unroll
             for (int l = 0; l < LL; l++) {
-                sumr += pl[(3 + l) * P::PLS + pc];
-                sump += pl[(3 + LL + l) * P::PLS + pc];
-                sumq += pl[(3 + 2 * LL + l) * P::PLS + pc];
+                out.put(S.mem_off[0] + l * g.plane, o[3 + l][0], o[3 + l][1]);
+                out.put(S.mem_off[1] + l * g.plane, o[3 + LL + l][0], o[3 + LL + l][1]);
+                out.put(S.mem_off[2] + l * g.plane, o[3 + 2 * LL + l][0], o[3 + 2 * LL + l][1]);
             }
-            const T fipjp = pl[CO * P::PLS + pc], f = pl[(CO + 1) * P::PLS + pc], gg = pl[(CO + 2) * P::PLS + pc];
-            const T mu = pl[(CO + 3) * P::PLS + pc], pi = pl[(CO + 4) * P::PLS + pc],
-                    muij = pl[(CO + 5) * P::PLS + pc];
-            const T ts = ts_p ? ts_p[c] : (T)g.taus0, tp = tp_p ? tp_p[c] : (T)g.taup0,
-                    tsij = tsij_p ? tsij_p[c] : (T)g.tausipjp0;
-            const T s_xy = pl[2 * P::PLS + pc] + ((fipjp * (vxy + vyx)) + (dthalbe * sumr));
-            const T s_xx = (T)((D)pl[pc] + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vyy) + (D)(dthalbe * sump)));
-            const T s_yy =
-                (T)((D)pl[P::PLS + pc] + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vxx) + (D)(dthalbe * sumq)));
-            sumr = sump = sumq = 0;
-#pragma unroll
-            for (int l = 0; l < LL; l++) {
-                const T eta = g.eta[l + 1];
-                const T dip = muij * eta * tsij, dd = mu * eta * ts, e = pi * eta * tp;
-                const T rr = (T)g.bip[l + 1] * (pl[(3 + l) * P::PLS + pc] * (T)g.cip[l + 1] - (dip * (vxy + vyx)));
-                const T pp = (T)((D)g.bjm[l + 1] *
-                                 ((D)(pl[(3 + LL + l) * P::PLS + pc] * (T)g.cjm[l + 1] - (e * (vxx + vyy))) +
-                                  ((D)2 * (D)dd * (D)vyy)));
-                const T qq = (T)((D)g.bjm[l + 1] *
-                                 ((D)(pl[(3 + 2 * LL + l) * P::PLS + pc] * (T)g.cjm[l + 1] - (e * (vxx + vyy))) +
-                                  ((D)2 * (D)dd * (D)vxx)));
-                mr[c + l * PL] = rr;
-                mp[c + l * PL] = pp;
-                mq[c + l * PL] = qq;
-                sumr += rr;
-                sump += pp;
-                sumq += qq;
-            }
-            sxy[c] = s_xy + (dthalbe * sumr);
-            sxx[c] = s_xx + (dthalbe * sump);
-            syy[c] = s_yy + (dthalbe * sumq);
+            out.snap(so.n, tm.snap_comp[P_SXX], o[0][0], o[0][1]);
+            out.snap(so.n, tm.snap_comp[P_SYY], o[1][0], o[1][1]);
+            out.snap(so.n, tm.snap_comp[P_SXY], o[2][0], o[2][1]);
         }
     }
 };
 
-// stress, SH elastic (src/update_s_elastic_PML_SH.c); halo: vz; plain: sxz syz uipjp f
-template <typename T, int FDOH, int TY, int NST>
-struct OpSShEl {
-    using P = Pipe<T, FDOH, TY, 1, 4, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
+// stress, P-SV elastic (src/update_s_elastic_PML.c:151-241; 10/12: :442-535)
+// halo: vx vy; plain: sxx syy sxy uipjp f g (reference 10/12 branch: uipjp vs vp);
+// writes sxx syy sxy
+template <int FDOH, int TY, int NST, bool QUIRK>
+struct OpSEl {
+    static constexpr int NH_ = 2, NP_ = 6;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
-        hz[0] = zb + tm.pid[P_VZ];
-        pz[0] = {zb + tm.pid[P_SXZ], false};
-        pz[1] = {zb + tm.pid[P_SYZ], false};
-        pz[2] = {mb + tm.mid[M_UIPJP], true};
-        pz[3] = {mb + tm.mid[M_F], true};
+        const int mb = ti.model * tm.model_planes;
+        hz[0] = zb + tm.pid[P_VX];
+        hz[1] = zb + tm.pid[P_VY];
+        pz[0] = {zb + tm.pid[P_SXX], false};
+        pz[1] = {zb + tm.pid[P_SYY], false};
+        pz[2] = {zb + tm.pid[P_SXY], false};
+        pz[3] = {mb + tm.mid[M_UIPJP], true};
+        pz[4] = {mb + tm.mid[QUIRK ? M_VS : M_F], true};
+        pz[5] = {mb + tm.mid[QUIRK ? M_VP : M_G], true};
     }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        const T *t_vz = h;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ sxz = S.base + so + S.off[P_SXZ];
-        T *__restrict__ syz = S.base + so + S.off[P_SYZ];
-        T *ps_x = S.psix[X_VZX] + slot * S.psix_slot, *ps_y = S.psiy[Y_VZY] + slot * S.psiy_slot;
-        const T dhi = (T)g.dt / (T)g.dh;
+    IFOS_TILE_COMPUTE(QUIRK)
+    template <bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_vx = h, *t_vy = h + P::BOXS;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wx[RT], wy[RT];
+        float2 dxy[RT], dyy[RT], in[RT][NP_];
 #pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wx[r].load(t_vx + (jj + P::H) * P::BW, cl.c0);
+            wy[r].load(t_vy + (jj + P::H) * P::BW, cl.c0);
+            dxy[r] = yfwd2<false, false, P, FDOH>(hc, t_vx, jj, cl.c0);
+            dyy[r] = ybwd2<false, false, P, FDOH>(hc, t_vy, jj, cl.c0);
+#pragma unroll
+            for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const float DT = g.dt, DH = g.dh;
+        const float dhi = DT / DH;
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
             if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + tx + P::XH, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            T vzx = 0, vzy = 0;
+            float o[3][2];
 #pragma unroll
-            for (int m = 1; m <= FDOH; m++) vzx += hc.w[m] * (t_vz[rc + m] - t_vz[rc - m + 1]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) vzy += hc.w[m] * (t_vz[rc + (m - 1) * P::BW] - t_vz[rc - m * P::BW]);
-            vzx = vzx * dhi;
-            vzy = vzy * dhi;
-            vzx = cpml_xh(g, M, ps_x, j, hx, K_XH, A_XH, B_XH, vzx);
-            vzy = cpml_yh(g, M, ps_y, i, hy, K_Y, A_Y, B_Y, vzy);
-            sxz[c] = pl[pc] + (pl[2 * P::PLS + pc] * vzx);
-            syz[c] = pl[P::PLS + pc] + (pl[3 * P::PLS + pc] * vzy);
+            for (int e = 0; e < 2; e++) {
+                const float2 *v = in[r];
+                float vxx = xbwd<FDOH, P::HE>(hc, wx[r], e) * dhi;
+                float vyx = xfwd<FDOH, P::HE>(hc, wy[r], e) * dhi;
+                float vxy = pick(dxy[r], e) * dhi, vyy = pick(dyy[r], e) * dhi;
+                const float sxx0 = pick(v[0], e), syy0 = pick(v[1], e), sxy0 = pick(v[2], e);
+                if (QUIRK) {
+                    const float fipjp = pick(v[3], e) * DT, f = pick(v[4], e) * DT, gg = pick(v[5], e) * DT;
+                    o[2][e] = sxy0 + (fipjp * (vxy + vyx));
+                    o[0][e] = (float)((D)sxx0 + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vyy)));
+                    o[1][e] = (float)((D)syy0 + ((D)(gg * (vxx + vyy)) - ((D)2 * (D)f * (D)vxx)));
+                    continue;
+                }
+                if (PML && cl.valid(e)) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) {
+                        vxx = pml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, vxx);
+                        vyx = pml_x(g, M, S.psix[X_VYX] + slot * S.psix_slot, j, hx, K_XH, A_XH, B_XH, vyx);
+                    }
+                    const int hy = strip_y(g, j);
+                    if (hy) {
+                        vyy = pml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, vyy);
+                        vxy = pml_y(g, M, S.psiy[Y_VXY] + slot * S.psiy_slot, ii, hy, K_YH, A_YH, B_YH, vxy);
+                    }
+                }
+                const float fipjp = pick(v[3], e), f = pick(v[4], e), gg = pick(v[5], e);
+                o[2][e] = sxy0 + fipjp * (vyx + vxy);
+                o[0][e] = (float)((D)sxx0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vxx)));
+                o[1][e] = (float)((D)syy0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vyy)));
+            }
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_SXX], o[0][0], o[0][1]);
+            out.put(S.off[P_SYY], o[1][0], o[1][1]);
+            out.put(S.off[P_SXY], o[2][0], o[2][1]);
+            out.snap(so.n, tm.snap_comp[P_SXX], o[0][0], o[0][1]);
+            out.snap(so.n, tm.snap_comp[P_SYY], o[1][0], o[1][1]);
+            out.snap(so.n, tm.snap_comp[P_SXY], o[2][0], o[2][1]);
         }
     }
 };
 
-// stress, SH viscoelastic (src/update_s_visc_PML_SH.c); halo: vz;
-// plain: sxz syz t[LL] o[LL] fipjp f mu muipjp
-template <typename T, int FDOH, int TY, int LL, int NST>
-struct OpSShVisc {
-    static constexpr int NP = 2 + 2 * LL + 4;
-    using P = Pipe<T, FDOH, TY, 1, NP, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
+// ---------------------------------------------------------------------------
+// velocity, P-SV (src/update_v_PML.c:161-252; 10/12 reference branches
+// :466-528 when QUIRK) and acoustic (src/update_v_acoustic_PML.c:72-148,
+// default :396-409 when QUIRK; AC).  halo: sxx syy sxy (acoustic: sp);
+// plain: vx vy rip rjp [+ vxp1 vyp1 in the adjoint].  SW: 0 forward,
+// 1 adjoint; P1: this forward step forms vxp1/vyp1 for a snapshot (written to
+// the snapshot when the launch stores one, else to the state).
+template <int FDOH, int TY, int NST, bool QUIRK, int SW, bool P1, bool AC>
+struct OpVPsv {
+    static constexpr int NH_ = AC ? 1 : 3;
+    static constexpr int NP_ = (SW == 1 && !QUIRK) ? 6 : 4;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
+        const int mb = ti.model * tm.model_planes;
+        if (AC) {
+            hz[0] = zb + tm.pid[P_SP];
+        } else {
+            hz[0] = zb + tm.pid[P_SXX];
+            hz[(1 < NH_) ? 1 : 0] = zb + tm.pid[P_SYY];
+            hz[(2 < NH_) ? 2 : 0] = zb + tm.pid[P_SXY];
+        }
+        pz[0] = {zb + tm.pid[P_VX], false};
+        pz[1] = {zb + tm.pid[P_VY], false};
+        pz[2] = {mb + tm.mid[M_RIP], true};
+        pz[3] = {mb + tm.mid[M_RJP], true};
+        if (NP_ > 4) {
+            pz[4 % NP_] = {zb + tm.pid[P_VXP1], false};
+            pz[5 % NP_] = {zb + tm.pid[P_VYP1], false};
+        }
+    }
+    __device__ __forceinline__ void compute(const TileInfo &ti, const float *h, const float *pl,
+                                            uint64_t *empty) const {
+        const Cols cl(g, ti, P::XH, !QUIRK);
+        const bool mir = g.free_surf && ti.j0 == 1;
+        if (QUIRK || (cl.hx0 == 0 && cl.hx1 == 0 && !ti.ystrip)) {
+            if (mir) rows<true, false>(ti, cl, h, pl, empty);
+            else rows<false, false>(ti, cl, h, pl, empty);
+        } else {
+            if (mir) rows<true, true>(ti, cl, h, pl, empty);
+            else rows<false, true>(ti, cl, h, pl, empty);
+        }
+    }
+    template <bool MIR, bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        // P-SV: sxx, syy, sxy boxes; acoustic: the sp box serves as all three
+        const float *t_sxx = h, *t_syy = AC ? h : h + P::BOXS, *t_sxy = AC ? h : h + 2 * P::BOXS;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wxx[RT], wxy[RT];
+        float2 dyy[RT], dxy[RT], in[RT][NP_];
+        float2 qa[RT][QUIRK && !AC ? FDOH : 1];  // reference 10/12 P-SV form: the sxy y-taps one by one
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wxx[r].load(t_sxx + (jj + P::H) * P::BW, cl.c0);
+            if (!AC) wxy[r].load(t_sxy + (jj + P::H) * P::BW, cl.c0);
+            dyy[r] = yfwd2<MIR, false, P, FDOH, QUIRK && AC>(hc, t_syy, jj, cl.c0);
+            if (!AC && !QUIRK) dxy[r] = ybwd2<MIR, true, P, FDOH>(hc, t_sxy, jj, cl.c0);
+            if (!AC && QUIRK) {
+#pragma unroll
+                for (int m = 1; m <= (QUIRK && !AC ? FDOH : 1); m++) {
+                    const float2 a = ldy2<MIR, true, P>(t_sxy, jj, cl.c0, m - 1);
+                    const float2 b = ldy2<MIR, true, P>(t_sxy, jj, cl.c0, -m);
+                    qa[r][m - 1] = make_float2(a.x - b.x, a.y - b.y);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const float DT = g.dt, DH = g.dh;
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
+            if (j > g.ny) break;
+            float o[4][2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const float2 *v = in[r];
+                const float vxo = pick(v[0], e), vyo = pick(v[1], e), rip = pick(v[2], e), rjp = pick(v[3], e);
+                float a_x, a_y, b_x = 0.0f, b_y = 0.0f;  // P-SV: sxx_x, syy_y, sxy_x, sxy_y; acoustic: sp_x, sp_y
+                if (QUIRK) {
+                    const float dtdh = DT * DT / DH;
+                    if (AC) {
+                        a_x = xfwd<FDOH, P::HE, true>(hc, wxx[r], e);
+                        a_y = pick(dyy[r], e);
+                    } else {
+                        // one written-out sum per component (src/update_v_PML.c:469-490)
+                        a_x = xfwd<FDOH, P::HE>(hc, wxx[r], e);
+#pragma unroll
+                        for (int m = 1; m <= (QUIRK && !AC ? FDOH : 1); m++) a_x += hc.w[m] * pick(qa[r][m - 1], e);
+                        a_y = pick(dyy[r], e);
+#pragma unroll
+                        for (int m = 1; m <= FDOH; m++)
+                            a_y += hc.w[m] * (wxy[r].v[P::HE + e + m - 1] - wxy[r].v[P::HE + e - m]);
+                    }
+                    o[0][e] = vxo + a_x * dtdh * rip;
+                    o[1][e] = vyo + a_y * dtdh * rjp;
+                    continue;
+                }
+                a_x = xfwd<FDOH, P::HE>(hc, wxx[r], e);
+                a_y = pick(dyy[r], e);
+                if (!AC) {
+                    b_x = xbwd<FDOH, P::HE>(hc, wxy[r], e);
+                    b_y = pick(dxy[r], e);
+                }
+                if (PML && cl.valid(e)) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) {
+                        a_x = pml_x(g, M, S.psix[X_SXX] + slot * S.psix_slot, j, hx, K_XH, A_XH, B_XH, a_x);
+                        if (!AC) b_x = pml_x(g, M, S.psix[X_SXY] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, b_x);
+                    }
+                    const int hy = strip_y(g, j);
+                    if (hy) {
+                        a_y = pml_y(g, M, S.psiy[Y_SYY] + slot * S.psiy_slot, ii, hy, K_YH, A_YH, B_YH, a_y);
+                        if (!AC) b_y = pml_y(g, M, S.psiy[Y_SXY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, b_y);
+                    }
+                }
+                // P-SV: x force sxx_x + sxy_y, y force sxy_x + syy_y; acoustic: sp_x, sp_y
+                const float fx = AC ? (a_x) : (a_x + b_y), fy = AC ? (a_y) : (b_x + a_y);
+                if (SW == 0) {
+                    if (P1) {
+                        o[2][e] = div_dh(g, rip * fx);
+                        o[3][e] = div_dh(g, rjp * fy);
+                    }
+                } else {
+                    o[2][e] = pick(v[4 % NP_], e) + vxo * DT;
+                    o[3][e] = pick(v[5 % NP_], e) + vyo * DT;
+                }
+                o[0][e] = vxo + div_dh(g, DT * rip * fx);
+                o[1][e] = vyo + div_dh(g, DT * rjp * fy);
+            }
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_VX], o[0][0], o[0][1]);
+            out.put(S.off[P_VY], o[1][0], o[1][1]);
+            if (!QUIRK && (SW == 1 || (P1 && !out.sn))) {
+                out.put(S.off[P_VXP1], o[2][0], o[2][1]);
+                out.put(S.off[P_VYP1], o[3][0], o[3][1]);
+            }
+            if (!QUIRK && SW == 0 && P1) {
+                out.snap(so.n, tm.snap_comp[P_VXP1], o[2][0], o[2][1]);
+                out.snap(so.n, tm.snap_comp[P_VYP1], o[3][0], o[3][1]);
+            }
+        }
+    }
+};
+
+// velocity, SH (src/update_v_PML_SH.c:61-297, CPML on every order);
+// halo: sxz syz; plain: vz rjp; writes vz and vzp1 = previous vz
+template <int FDOH, int TY, int NST>
+struct OpVSh {
+    static constexpr int NH_ = 2, NP_ = 2;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
+        const int zb = ti.slot * tm.planes_per_slot;
+        const int mb = ti.model * tm.model_planes;
+        hz[0] = zb + tm.pid[P_SXZ];
+        hz[1] = zb + tm.pid[P_SYZ];
+        pz[0] = {zb + tm.pid[P_VZ], false};
+        pz[1] = {mb + tm.mid[M_RJP], true};
+    }
+    __device__ __forceinline__ void compute(const TileInfo &ti, const float *h, const float *pl,
+                                            uint64_t *empty) const {
+        const Cols cl(g, ti, P::XH, true);
+        const bool mir = g.free_surf && ti.j0 == 1;
+        if (cl.hx0 == 0 && cl.hx1 == 0 && !ti.ystrip) {
+            if (mir) rows<true, false>(ti, cl, h, pl, empty);
+            else rows<false, false>(ti, cl, h, pl, empty);
+        } else {
+            if (mir) rows<true, true>(ti, cl, h, pl, empty);
+            else rows<false, true>(ti, cl, h, pl, empty);
+        }
+    }
+    template <bool MIR, bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_sxz = h, *t_syz = h + P::BOXS;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wxz[RT];
+        float2 dyz[RT], vz2[RT], rjp2[RT];
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wxz[r].load(t_sxz + (jj + P::H) * P::BW, cl.c0);
+            dyz[r] = yfwd2<MIR, false, P, FDOH>(hc, t_syz, jj, cl.c0);
+            vz2[r] = lds2(pl + jj * kTileX + 2 * cl.lane);
+            rjp2[r] = lds2(pl + P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const float DT = g.dt;
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
+            if (j > g.ny) break;
+            float o[2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                float sxz_x = xbwd<FDOH, P::HE>(hc, wxz[r], e), syz_y = pick(dyz[r], e);
+                if (PML && cl.valid(e)) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) sxz_x = pml_x(g, M, S.psix[X_SXZ] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, sxz_x);
+                    const int hy = strip_y(g, j);
+                    if (hy) syz_y = pml_y(g, M, S.psiy[Y_SYZ] + slot * S.psiy_slot, ii, hy, K_YH, A_YH, B_YH, syz_y);
+                }
+                o[e] = pick(vz2[r], e) + div_dh(g, pick(rjp2[r], e) * DT * (sxz_x + syz_y));
+            }
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_VZP1], vz2[r].x, vz2[r].y);
+            out.put(S.off[P_VZ], o[0], o[1]);
+            out.snap(so.n, tm.snap_comp[P_VZP1], vz2[r].x, vz2[r].y);
+        }
+    }
+};
+
+// stress, SH elastic / viscoelastic (src/update_s_elastic_PML_SH.c,
+// src/update_s_visc_PML_SH.c); halo: vz; plain: sxz syz [t[LL] o[LL]] and the
+// coefficients (elastic: uipjp f; visco: fipjp f mu muipjp); writes sxz syz [t o]
+template <int FDOH, int TY, int LL, int NST>
+struct OpSSh {
+    static constexpr int NH_ = 1, NP_ = LL ? 2 + 2 * LL + 4 : 4, NOUT = 2 + 2 * LL;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
+        const int zb = ti.slot * tm.planes_per_slot;
+        const int mb = ti.model * tm.model_planes;
         hz[0] = zb + tm.pid[P_VZ];
         pz[0] = {zb + tm.pid[P_SXZ], false};
         pz[1] = {zb + tm.pid[P_SYZ], false};
+        if (LL == 0) {
+            pz[2] = {mb + tm.mid[M_UIPJP], true};
+            pz[3] = {mb + tm.mid[M_F], true};
+        } else {
 #pragma unroll
-        for (int l = 0; l < LL; l++) {
-            pz[2 + l] = {zb + tm.mem_pid[3] + l, false};       // t
-            pz[2 + LL + l] = {zb + tm.mem_pid[4] + l, false};  // o
+            for (int l = 0; l < LL; l++) {
+                pz[(2 + l) % NP_] = {zb + tm.mem_pid[3] + l, false};       // t
+                pz[(2 + LL + l) % NP_] = {zb + tm.mem_pid[4] + l, false};  // o
+            }
+            pz[(2 + 2 * LL + 0) % NP_] = {mb + tm.mid[M_FIPJPV], true};
+            pz[(2 + 2 * LL + 1) % NP_] = {mb + tm.mid[M_FV], true};
+            pz[(2 + 2 * LL + 2) % NP_] = {mb + tm.mid[M_MUR], true};
+            pz[(2 + 2 * LL + 3) % NP_] = {mb + tm.mid[M_MUIPJPR], true};
         }
-        pz[2 + 2 * LL + 0] = {mb + tm.mid[M_FIPJPV], true};
-        pz[2 + 2 * LL + 1] = {mb + tm.mid[M_FV], true};
-        pz[2 + 2 * LL + 2] = {mb + tm.mid[M_MUR], true};
-        pz[2 + 2 * LL + 3] = {mb + tm.mid[M_MUIPJPR], true};
     }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        const T *t_vz = h;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        const long long mo = (long long)model * M.model_stride;
-        T *__restrict__ sxz = S.base + so + S.off[P_SXZ];
-        T *__restrict__ syz = S.base + so + S.off[P_SYZ];
-        T *__restrict__ mt = S.base + so + S.mem_off[3];
-        T *__restrict__ mo_ = S.base + so + S.mem_off[4];
-        T *ps_x = S.psix[X_VZX] + slot * S.psix_slot, *ps_y = S.psiy[Y_VZY] + slot * S.psiy_slot;
-        const T *ts_p = M.m[M_TAUS] ? M.m[M_TAUS] + mo : nullptr,
-                *tsij_p = M.m[M_TAUSIPJP] ? M.m[M_TAUSIPJP] + mo : nullptr;
-        const long long PL = g.plane;
-        const T DT = g.dt, DH = g.dh;
-        const T dhi = (T)(1.0 / (double)DH), dthalbe = (T)((double)DT / 2.0);
+    IFOS_TILE_COMPUTE(false)
+    template <bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_vz = h;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wz[RT];
+        float2 dzy[RT], in[RT][NP_];
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wz[r].load(t_vz + (jj + P::H) * P::BW, cl.c0);
+            dzy[r] = ybwd2<false, false, P, FDOH>(hc, t_vz, jj, cl.c0);
+#pragma unroll
+            for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const long long mo = (long long)ti.model * M.model_stride;
+        const float *ts_p = M.m[M_TAUS] ? M.m[M_TAUS] + mo : nullptr;
+        const float *tsij_p = M.m[M_TAUSIPJP] ? M.m[M_TAUSIPJP] + mo : nullptr;
+        const float DT = g.dt, DH = g.dh;
+        const float dhi = LL ? (float)(1.0 / (double)DH) : DT / DH, dthalbe = (float)((double)DT / 2.0);
         constexpr int CO = 2 + 2 * LL;
 #pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
             if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + tx + P::XH, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            T vzx = 0, vzy = 0;
+            float o[NOUT][2];
 #pragma unroll
-            for (int m = 1; m <= FDOH; m++) vzx += hc.w[m] * (t_vz[rc + m] - t_vz[rc - m + 1]);
+            for (int e = 0; e < 2; e++) {
+                const float2 *v = in[r];
+                float vzx = xfwd<FDOH, P::HE>(hc, wz[r], e) * dhi, vzy = pick(dzy[r], e) * dhi;
+                const bool ok = cl.valid(e);
+                if (PML && ok) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) vzx = pml_x(g, M, S.psix[X_VZX] + slot * S.psix_slot, j, hx, K_XH, A_XH, B_XH, vzx);
+                    const int hy = strip_y(g, j);
+                    if (hy) vzy = pml_y(g, M, S.psiy[Y_VZY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, vzy);
+                }
+                if (LL == 0) {
+                    o[0][e] = pick(v[0], e) + (pick(v[2], e) * vzx);
+                    o[1][e] = pick(v[1], e) + (pick(v[3], e) * vzy);
+                    continue;
+                }
+                float sumo = 0, sumt = 0;
 #pragma unroll
-            for (int m = 1; m <= FDOH; m++) vzy += hc.w[m] * (t_vz[rc + (m - 1) * P::BW] - t_vz[rc - m * P::BW]);
-            vzx = vzx * dhi;
-            vzy = vzy * dhi;
-            vzx = cpml_xh(g, M, ps_x, j, hx, K_XH, A_XH, B_XH, vzx);
-            vzy = cpml_yh(g, M, ps_y, i, hy, K_Y, A_Y, B_Y, vzy);
-            T sumo = 0, sumt = 0;
+                for (int l = 0; l < LL; l++) {
+                    sumo += pick(v[(2 + LL + l) % NP_], e);
+                    sumt += pick(v[(2 + l) % NP_], e);
+                }
+                const float fipjp = pick(v[CO % NP_], e), f = pick(v[(CO + 1) % NP_], e);
+                const float mu = pick(v[(CO + 2) % NP_], e), muij = pick(v[(CO + 3) % NP_], e);
+                float ts = g.taus0, tsij = g.tausipjp0;
+                if (ok && (ts_p || tsij_p)) {
+                    const int c = (j - 1 + HY) * g.pitch + (cl.i + e - 1 + HX);
+                    if (ts_p) ts = ts_p[c];
+                    if (tsij_p) tsij = tsij_p[c];
+                }
+                const float s_xz = pick(v[0], e) + ((fipjp * vzx) + (dthalbe * sumo));
+                const float s_yz = pick(v[1], e) + ((f * vzy) + (dthalbe * sumt));
+                sumo = sumt = 0;
+#pragma unroll
+                for (int l = 0; l < LL; l++) {
+                    const float eta = g.eta[l + 1];
+                    const float dip = muij * eta * tsij, dd = mu * eta * ts;
+                    const float oo = g.bip[l + 1] * (pick(v[(2 + LL + l) % NP_], e) * g.cip[l + 1] - (dip * vzx));
+                    const float tt = g.bjm[l + 1] * (pick(v[(2 + l) % NP_], e) * g.cjm[l + 1] - (dd * vzy));
+                    o[(2 + LL + l) % NOUT][e] = oo;
+                    o[(2 + l) % NOUT][e] = tt;
+                    sumt += tt;
+                    sumo += oo;
+                }
+                o[0][e] = s_xz + (dthalbe * sumo);
+                o[1][e] = s_yz + (dthalbe * sumt);
+            }
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_SXZ], o[0][0], o[0][1]);
+            out.put(S.off[P_SYZ], o[1][0], o[1][1]);
 #pragma unroll
             for (int l = 0; l < LL; l++) {
-                sumo += pl[(2 + LL + l) * P::PLS + pc];
-                sumt += pl[(2 + l) * P::PLS + pc];
+                out.put(S.mem_off[3] + l * g.plane, o[(2 + l) % NOUT][0], o[(2 + l) % NOUT][1]);
+                out.put(S.mem_off[4] + l * g.plane, o[(2 + LL + l) % NOUT][0], o[(2 + LL + l) % NOUT][1]);
             }
-            const T fipjp = pl[CO * P::PLS + pc], f = pl[(CO + 1) * P::PLS + pc];
-            const T mu = pl[(CO + 2) * P::PLS + pc], muij = pl[(CO + 3) * P::PLS + pc];
-            const T ts = ts_p ? ts_p[c] : (T)g.taus0, tsij = tsij_p ? tsij_p[c] : (T)g.tausipjp0;
-            const T s_xz = pl[pc] + ((fipjp * vzx) + (dthalbe * sumo));
-            const T s_yz = pl[P::PLS + pc] + ((f * vzy) + (dthalbe * sumt));
-            sumo = sumt = 0;
-#pragma unroll
-            for (int l = 0; l < LL; l++) {
-                const T eta = g.eta[l + 1];
-                const T dip = muij * eta * tsij, dd = mu * eta * ts;
-                const T o = (T)g.bip[l + 1] * (pl[(2 + LL + l) * P::PLS + pc] * (T)g.cip[l + 1] - (dip * vzx));
-                const T t = (T)g.bjm[l + 1] * (pl[(2 + l) * P::PLS + pc] * (T)g.cjm[l + 1] - (dd * vzy));
-                mo_[c + l * PL] = o;
-                mt[c + l * PL] = t;
-                sumt += t;
-                sumo += o;
-            }
-            sxz[c] = s_xz + (dthalbe * sumo);
-            syz[c] = s_yz + (dthalbe * sumt);
+            out.snap(so.n, tm.snap_comp[P_SXZ], o[0][0], o[0][1]);
+            out.snap(so.n, tm.snap_comp[P_SYZ], o[1][0], o[1][1]);
         }
     }
 };
 
-// pressure, acoustic (src/update_p_PML.c:55-273; default :275-287)
-// halo: vx vy; plain: sp g (reference 10/12 branch: vp)
-template <typename T, int FDOH, int TY, int NST>
+// pressure, acoustic (src/update_p_PML.c:55-273; default :275-287 when QUIRK)
+// halo: vx vy; plain: sp g (reference 10/12 branch: vp); writes sp
+template <int FDOH, int TY, int NST, bool QUIRK>
 struct OpPAc {
-    using P = Pipe<T, FDOH, TY, 2, 2, NST>;
-    KGrid g;
-    KState<T> S;
-    KModel<T> M;
-    KTma tm;
-    __device__ void planes(const TileIdx &ti, int model, int *hz, PlainSrc *pz) const {
+    static constexpr int NH_ = 2, NP_ = 2;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
-        const int mb = model * tm.model_planes;
+        const int mb = ti.model * tm.model_planes;
         hz[0] = zb + tm.pid[P_VX];
         hz[1] = zb + tm.pid[P_VY];
         pz[0] = {zb + tm.pid[P_SP], false};
-        pz[1] = {mb + tm.mid[g.quirk_hi ? M_VP : M_GAC], true};
+        pz[1] = {mb + tm.mid[QUIRK ? M_VP : M_GAC], true};
     }
-    __device__ void compute(const TileIdx &ti, int model, T *h, const T *pl) const {
-        const T *t_vx = h, *t_vy = h + P::BOXS;
-        const int tx = threadIdx.x, i = ti.i0 + tx, slot = ti.slot;
-        if (i > g.nx) return;
-        const int hx = strip_x(g, i);
-        const Hc<T, FDOH> hc(g);
-        const long long so = (long long)slot * S.slot_stride;
-        T *__restrict__ sp = S.base + so + S.off[P_SP];
-        T *ps_x = S.psix[X_VXX] + slot * S.psix_slot, *ps_y = S.psiy[Y_VYY] + slot * S.psiy_slot;
-        const T DT = g.dt, DH = g.dh;
-        const T dhi = DT / DH;
+    IFOS_TILE_COMPUTE(QUIRK)
+    template <bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_vx = h, *t_vy = h + P::BOXS;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wx[RT];
+        float2 dyy[RT], sp2[RT], g2[RT];
 #pragma unroll
-        for (int r = 0; r < P::RT; r++) {
-            const int jj = threadIdx.y + 8 * r, j = ti.j0 + jj;
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wx[r].load(t_vx + (jj + P::H) * P::BW, cl.c0);
+            dyy[r] = ybwd2<false, false, P, FDOH, QUIRK>(hc, t_vy, jj, cl.c0);
+            sp2[r] = lds2(pl + jj * kTileX + 2 * cl.lane);
+            g2[r] = lds2(pl + P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const float DT = g.dt, DH = g.dh;
+        const float dhi = DT / DH;
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
             if (j > g.ny) break;
-            const int hy = strip_y(g, j);
-            const int rc = (jj + P::H) * P::BW + tx + P::XH, pc = jj * 32 + tx;
-            const int c = (int)pidx(g, j, i);
-            T vxx = 0, vyy = 0;
+            float o[2];
 #pragma unroll
-            for (int m = 1; m <= FDOH; m++) vxx += hc.w[m] * (t_vx[rc + m - 1] - t_vx[rc - m]);
-#pragma unroll
-            for (int m = 1; m <= FDOH; m++) vyy += hc.w[m] * (t_vy[rc + (m - 1) * P::BW] - t_vy[rc - m * P::BW]);
-            if (g.quirk_hi) {
-                const T gg = pl[P::PLS + pc] * DT;
-                sp[c] = pl[pc] + (gg * (vxx + vyy)) * dhi;
-                continue;
+            for (int e = 0; e < 2; e++) {
+                float vxx = xbwd<FDOH, P::HE, QUIRK>(hc, wx[r], e), vyy = pick(dyy[r], e);
+                if (QUIRK) {
+                    const float gg = pick(g2[r], e) * DT;
+                    o[e] = pick(sp2[r], e) + (gg * (vxx + vyy)) * dhi;
+                    continue;
+                }
+                vxx = vxx * dhi;
+                vyy = vyy * dhi;
+                if (PML && cl.valid(e)) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) vxx = pml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, vxx);
+                    const int hy = strip_y(g, j);
+                    if (hy) vyy = pml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, vyy);
+                }
+                o[e] = pick(sp2[r], e) + pick(g2[r], e) * (vxx + vyy);
             }
-            vxx = vxx * dhi;
-            vyy = vyy * dhi;
-            vxx = cpml_xh(g, M, ps_x, j, hx, K_X, A_X, B_X, vxx);
-            vyy = cpml_yh(g, M, ps_y, i, hy, K_Y, A_Y, B_Y, vyy);
-            sp[c] = pl[pc] + pl[P::PLS + pc] * (vxx + vyy);
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_SP], o[0], o[1]);
+            out.snap(so.n, tm.snap_comp[P_SP], o[0], o[1]);
         }
     }
 };
+#undef IFOS_TILE_COMPUTE
+#undef IFOS_OP_MEMBERS
+
+// Blocks per SM for the register budget: as many as the shared-memory ring
+// allows (227 KB per SM), at most 3, and no more than leave 64 registers a
+// thread.
+template <typename P>
+constexpr int ring_blocks() {
+    constexpr int by_smem = (int)(232448 / (P::bytes() + 1024));
+    constexpr int by_regs = 65536 / (kBlockThreads * 64);
+    constexpr int b = by_smem < by_regs ? by_smem : by_regs;
+    return b < 1 ? 1 : (b > 3 ? 3 : b);
+}
 
 // the kernel: one Op per launch, persistent over all tiles of all slots
-template <typename T, int FDOH, int TY, int NH, int NP, int NST, typename Op>
-__global__ void __launch_bounds__(kBlockThreads) kp_stencil(const __grid_constant__ KMaps maps,
-                                                            const __grid_constant__ Op op, int nshots, int *err) {
-    run_pipeline<T, FDOH, TY, NH, NP, NST>(op.g, maps, nshots, op, op.M.slot_model, err);
+template <typename Op>
+__global__ void __launch_bounds__(kBlockThreads, ring_blocks<typename Op::P>())
+    kp_stencil(const __grid_constant__ KMaps maps, const __grid_constant__ Op op, int nshots, int *err) {
+    run_pipeline<typename Op::P>(op.g, maps, nshots, op, err);
 }
 
 }  // namespace ifos

@@ -417,23 +417,49 @@ static inline float cpml(float *psi, float b, float a, float K, float d) {
     } while (0)
 
 /* staggered first differences: forward (+) reads f[k+m] - f[k-m+1],
- * backward (-) reads f[k+m-1] - f[k-m]; summed in the reference's order */
+ * backward (-) reads f[k+m-1] - f[k-m]; summed in the reference's order,
+ * the m=1 term starting the sum as in its written-out expressions
+ * (src/update_v_PML.c:164-175) */
 static inline float dfx_fwd(const grid_t *g, const float *f, int j, int i) {
+    float s = g->hc[1] * (A(f, j, i + 1) - A(f, j, i));
+    for (int m = 2; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j, i + m) - A(f, j, i - m + 1));
+    return s;
+}
+static inline float dfx_bwd(const grid_t *g, const float *f, int j, int i) {
+    float s = g->hc[1] * (A(f, j, i) - A(f, j, i - 1));
+    for (int m = 2; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j, i + m - 1) - A(f, j, i - m));
+    return s;
+}
+static inline float dfy_fwd(const grid_t *g, const float *f, int j, int i) {
+    float s = g->hc[1] * (A(f, j + 1, i) - A(f, j, i));
+    for (int m = 2; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j + m, i) - A(f, j - m + 1, i));
+    return s;
+}
+static inline float dfy_bwd(const grid_t *g, const float *f, int j, int i) {
+    float s = g->hc[1] * (A(f, j, i) - A(f, j - 1, i));
+    for (int m = 2; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j + m - 1, i) - A(f, j - m, i));
+    return s;
+}
+
+/* the same sums accumulated from zero, as the reference's generic loops do
+ * (its FDORDER 10/12 default branches: src/update_v_acoustic_PML.c:396-409,
+ * src/update_p_PML.c:275-287, src/update_s_visc_PML.c:615-660) */
+static inline float dfx_fwd_z(const grid_t *g, const float *f, int j, int i) {
     float s = 0.0f;
     for (int m = 1; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j, i + m) - A(f, j, i - m + 1));
     return s;
 }
-static inline float dfx_bwd(const grid_t *g, const float *f, int j, int i) {
+static inline float dfx_bwd_z(const grid_t *g, const float *f, int j, int i) {
     float s = 0.0f;
     for (int m = 1; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j, i + m - 1) - A(f, j, i - m));
     return s;
 }
-static inline float dfy_fwd(const grid_t *g, const float *f, int j, int i) {
+static inline float dfy_fwd_z(const grid_t *g, const float *f, int j, int i) {
     float s = 0.0f;
     for (int m = 1; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j + m, i) - A(f, j - m + 1, i));
     return s;
 }
-static inline float dfy_bwd(const grid_t *g, const float *f, int j, int i) {
+static inline float dfy_bwd_z(const grid_t *g, const float *f, int j, int i) {
     float s = 0.0f;
     for (int m = 1; m <= g->fdoh; m++) s += g->hc[m] * (A(f, j + m - 1, i) - A(f, j - m, i));
     return s;
@@ -450,10 +476,9 @@ static void update_v_psv(const grid_t *g, shot_t *s, int sw) {
     for (int j = 1; j <= g->ny; j++)
         for (int i = 1; i <= g->nx; i++) {
             if (quirk_hi(g)) {
-                float ax_ = 0.0f, ay_ = 0.0f;
-                for (int m = 1; m <= g->fdoh; m++) ax_ += g->hc[m] * (A(s->sxx, j, i + m) - A(s->sxx, j, i - m + 1));
+                /* one written-out sum per component (src/update_v_PML.c:469-490) */
+                float ax_ = dfx_fwd(g, s->sxx, j, i), ay_ = dfy_fwd(g, s->syy, j, i);
                 for (int m = 1; m <= g->fdoh; m++) ax_ += g->hc[m] * (A(s->sxy, j + m - 1, i) - A(s->sxy, j - m, i));
-                for (int m = 1; m <= g->fdoh; m++) ay_ += g->hc[m] * (A(s->syy, j + m, i) - A(s->syy, j - m + 1, i));
                 for (int m = 1; m <= g->fdoh; m++) ay_ += g->hc[m] * (A(s->sxy, j, i + m - 1) - A(s->sxy, j, i - m));
                 A(s->vx, j, i) += ax_ * dtdh * A(s->rip, j, i);
                 A(s->vy, j, i) += ay_ * dtdh * A(s->rjp, j, i);
@@ -500,9 +525,10 @@ static void update_v_ac(const grid_t *g, shot_t *s, int sw) {
     const float dtdh = DT * DT / DH;
     for (int j = 1; j <= g->ny; j++)
         for (int i = 1; i <= g->nx; i++) {
-            float sp_x = dfx_fwd(g, s->sp, j, i);
-            float sp_y = dfy_fwd(g, s->sp, j, i);
-            if (quirk_hi(g)) {
+            const int q = quirk_hi(g);
+            float sp_x = q ? dfx_fwd_z(g, s->sp, j, i) : dfx_fwd(g, s->sp, j, i);
+            float sp_y = q ? dfy_fwd_z(g, s->sp, j, i) : dfy_fwd(g, s->sp, j, i);
+            if (q) {
                 A(s->vx, j, i) += sp_x * dtdh * A(s->rip, j, i);
                 A(s->vy, j, i) += sp_y * dtdh * A(s->rjp, j, i);
                 continue;
@@ -602,11 +628,12 @@ static void update_s_psv_visc(const grid_t *g, shot_t *s) {
     const float dhi = 1.0 / DH, dthalbe = DT / 2.0;
     for (int j = 1; j <= g->ny; j++)
         for (int i = 1; i <= g->nx; i++) {
-            float vxx = dfx_bwd(g, s->vx, j, i) * dhi;
-            float vyx = dfx_fwd(g, s->vy, j, i) * dhi;
-            float vxy = dfy_fwd(g, s->vx, j, i) * dhi;
-            float vyy = dfy_bwd(g, s->vy, j, i) * dhi;
-            if (!(g->c.fdorder >= 10 && !g->c.hi_order_corrected)) {
+            const int q = quirk_hi(g);
+            float vxx = (q ? dfx_bwd_z(g, s->vx, j, i) : dfx_bwd(g, s->vx, j, i)) * dhi;
+            float vyx = (q ? dfx_fwd_z(g, s->vy, j, i) : dfx_fwd(g, s->vy, j, i)) * dhi;
+            float vxy = (q ? dfy_fwd_z(g, s->vx, j, i) : dfy_fwd(g, s->vx, j, i)) * dhi;
+            float vyy = (q ? dfy_bwd_z(g, s->vy, j, i) : dfy_bwd(g, s->vy, j, i)) * dhi;
+            if (!q) {
                 CPML_X(s->psi_vxx, j, i, g->bx, g->ax, g->Kx, vxx);
                 CPML_X(s->psi_vyx, j, i, g->bxh, g->axh, g->Kxh, vyx);
                 CPML_Y(s->psi_vyy, j, i, g->by, g->ay, g->Ky, vyy);
@@ -684,7 +711,7 @@ static void update_p_ac(const grid_t *g, shot_t *s) {
     for (int j = 1; j <= g->ny; j++)
         for (int i = 1; i <= g->nx; i++) {
             if (quirk_hi(g)) {
-                float vxx = dfx_bwd(g, s->vx, j, i), vyy = dfy_bwd(g, s->vy, j, i);
+                float vxx = dfx_bwd_z(g, s->vx, j, i), vyy = dfy_bwd_z(g, s->vy, j, i);
                 float gg = A(s->vp, j, i) * DT;
                 A(s->sp, j, i) += (gg * (vxx + vyy)) * dhi;
                 continue;
