@@ -12,6 +12,15 @@
 
 namespace ifos {
 
+// Programmatic dependent launch.  pdl_wait: block until the preceding kernel
+// of the stream has completed and its writes are visible (a no-op when this
+// kernel was not launched as a dependent); pdl_launch: let the next kernel
+// of the stream start its blocks before this one has finished.  Every kernel
+// the solver launches as a dependent calls pdl_wait before it touches memory
+// the preceding kernels write, and pdl_launch only after that wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // halo around every state plane (>= FDORDER/2 + 1 for FDORDER 12)
 constexpr int HX = 8;
 constexpr int HY = 8;
@@ -531,6 +540,8 @@ struct KRec {
 
 template <typename T>
 __global__ void k_inject_v_fwd(KGrid g, KState<T> S, KModel<T> M, KSrc src, int nt, int psv, int sh) {
+    pdl_wait();
+    pdl_launch();
     const int slot = blockIdx.x;
     if (threadIdx.x) return;
     const int n = src.nsrc[slot];
@@ -559,6 +570,8 @@ __global__ void k_inject_v_fwd(KGrid g, KState<T> S, KModel<T> M, KSrc src, int 
 
 template <typename T>
 __global__ void k_inject_v_adj(KGrid g, KState<T> S, KRec rec, int nt, int psv, int sh) {
+    pdl_wait();
+    pdl_launch();
     const int slot = blockIdx.y;
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= rec.ntr[slot]) return;
@@ -580,50 +593,48 @@ __global__ void k_inject_v_adj(KGrid g, KState<T> S, KRec rec, int nt, int psv, 
     if (sh) fieldp(S, slot, P_VZ)[c] += (T)adj[2 * cs + o];
 }
 
-// explosive source after the stress update (src/psource.c:37-58); one thread
-// per slot walks the sources in order
-template <typename T>
-__global__ void k_psource_fwd(KGrid g, KState<T> S, KSrc src, int nt, int acoustic, KSnapPatch pt) {
-    const int slot = blockIdx.x;
-    if (threadIdx.x) return;
+// Explosive source after the stress update (src/psource.c:37-58).
+// update_v_PML assigns the global SOURCE_TYPE from the type column of each
+// source it visits (src/update_v_PML.c:558); psource then fires when the last
+// one is explosive (src/IFOS2D.c:1758).
+__device__ __forceinline__ bool psource_fires(const KSrc &src, int slot) {
     const int n = src.nsrc[slot];
-    if (n <= 0) return;
+    if (n <= 0) return false;
     const float *pos = src.pos + (long long)slot * 8 * src.max_src;
-    // update_v_PML assigns the global SOURCE_TYPE from the type column of each
-    // source it visits (src/update_v_PML.c:558); psource then fires when the
-    // last one is explosive (src/IFOS2D.c:1758)
-    if ((int)pos[7 * src.max_src + n - 1] != 1) return;
+    return (int)pos[7 * src.max_src + n - 1] == 1;
+}
+// source l of a slot at its cell
+template <typename T>
+__device__ void psource_apply(const KGrid &g, const KState<T> &S, const KSrc &src, int nt, int acoustic,
+                              const KSnapPatch &pt, int slot, int l) {
+    const float *pos = src.pos + (long long)slot * 8 * src.max_src;
     const float *sig = src.sig + (long long)slot * src.max_src * src.nt_total;
     const int NT = src.nt_total;
     const float DH = g.dh;
-    for (int l = 0; l < n; l++) {
-        const int i = (int)pos[l], j = (int)pos[src.max_src + l];
-        const float *sl = sig + (long long)l * NT - 1;
-        float amp = 0.0f;
-        if (nt == 1) amp = sl[nt + 1] / (2.0 * DH * DH);
-        if ((nt > 1) && (nt < NT)) amp = (sl[nt + 1] - sl[nt - 1]) / (2.0 * DH * DH);
-        if (nt == NT) amp = -sl[nt - 1] / (2.0 * DH * DH);
-        const long long c = pidx(g, j, i);
-        if (!acoustic) {
-            T *sxx = fieldp(S, slot, P_SXX), *syy = fieldp(S, slot, P_SYY);
-            sxx[c] = (T)((double)sxx[c] + 0.5 * (double)amp);
-            syy[c] = (T)((double)syy[c] + 0.5 * (double)amp);
-            snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
-            snap_patch(pt, slot, pt.c_syy, g, j, i, (float)syy[c]);
-        } else {
-            T *sp = fieldp(S, slot, P_SP);
-            sp[c] += (T)amp;
-            snap_patch(pt, slot, pt.c_sp, g, j, i, (float)sp[c]);
-        }
+    const int i = (int)pos[l], j = (int)pos[src.max_src + l];
+    const float *sl = sig + (long long)l * NT - 1;
+    float amp = 0.0f;
+    if (nt == 1) amp = sl[nt + 1] / (2.0 * DH * DH);
+    if ((nt > 1) && (nt < NT)) amp = (sl[nt + 1] - sl[nt - 1]) / (2.0 * DH * DH);
+    if (nt == NT) amp = -sl[nt - 1] / (2.0 * DH * DH);
+    const long long c = pidx(g, j, i);
+    if (!acoustic) {
+        T *sxx = fieldp(S, slot, P_SXX), *syy = fieldp(S, slot, P_SYY);
+        sxx[c] = (T)((double)sxx[c] + 0.5 * (double)amp);
+        syy[c] = (T)((double)syy[c] + 0.5 * (double)amp);
+        snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
+        snap_patch(pt, slot, pt.c_syy, g, j, i, (float)syy[c]);
+    } else {
+        T *sp = fieldp(S, slot, P_SP);
+        sp[c] += (T)amp;
+        snap_patch(pt, slot, pt.c_sp, g, j, i, (float)sp[c]);
     }
 }
 
-// pressure residual at the receivers, ADJOINT_TYPE 4 (src/psource.c:61-74)
+// pressure residual at receiver l, ADJOINT_TYPE 4 (src/psource.c:61-74)
 template <typename T>
-__global__ void k_psource_adj(KGrid g, KState<T> S, KRec rec, int nt, int acoustic) {
-    const int slot = blockIdx.y;
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= rec.ntr[slot]) return;
+__device__ void psource_adj_rec(const KGrid &g, const KState<T> &S, const KRec &rec, int nt, int acoustic, int slot,
+                                int l) {
     const int *pos = rec.pos + (long long)slot * 2 * rec.max_rec;
     const long long c = pidx(g, pos[rec.max_rec + l], pos[l]);
     const float *adj = rec.adj + (long long)slot * 3 * rec.max_rec * g.nt_total;
@@ -641,10 +652,8 @@ __global__ void k_psource_adj(KGrid g, KState<T> S, KRec rec, int nt, int acoust
 // src/surface_PML.c:61-173, src/surface_acoustic_PML.c:28-38).  The mirrored
 // ghost rows are not stored: the velocity kernels read them via ld_mirror_*.
 template <typename T, int FDOH>
-__global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, int acoustic, KSnapPatch pt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int slot = blockIdx.y;
-    if (i > g.nx) return;
+__device__ void surface_cell(const KGrid &g, const KState<T> &S, const KModel<T> &M, int psv, int sh, int acoustic,
+                             const KSnapPatch &pt, int slot, int i) {
     const int j = 1;
     const long long c = pidx(g, j, i);
     if (acoustic) {
@@ -698,19 +707,18 @@ __global__ void k_surface(KGrid g, KState<T> S, KModel<T> M, int psv, int sh, in
     snap_patch(pt, slot, pt.c_sxx, g, j, i, (float)sxx[c]);
 }
 
-// receivers (src/seismo_ssg.c:26-140) and the instability probe of
-// src/IFOS2D.c:1660-1672 (vy or vz at the grid centre)
+// the instability probe of src/IFOS2D.c:1660-1672 (vy or vz at the grid centre)
+template <typename T>
+__device__ void nan_probe(const KGrid &g, const KState<T> &S, int psv, int slot, int *bad) {
+    const long long cc = pidx(g, g.ny / 2, g.nx / 2);
+    T v = psv ? fieldp(S, slot, P_VY)[cc] : fieldp(S, slot, P_VZ)[cc];
+    if (isnan((double)v)) atomicExch(bad, 1);
+}
+
+// receiver l (src/seismo_ssg.c:26-140)
 template <typename T, int FDOH>
-__global__ void k_seismo(KGrid g, KState<T> S, KModel<T> M, KRec rec, int nt, int seismo, int psv, int sh,
-                         int acoustic, int *bad) {
-    const int slot = blockIdx.y;
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l == 0) {
-        const long long cc = pidx(g, g.ny / 2, g.nx / 2);
-        T v = psv ? fieldp(S, slot, P_VY)[cc] : fieldp(S, slot, P_VZ)[cc];
-        if (isnan((double)v)) atomicExch(bad, 1);
-    }
-    if (l >= rec.ntr[slot] || !seismo) return;
+__device__ void seismo_rec(const KGrid &g, const KState<T> &S, const KModel<T> &M, const KRec &rec, int nt, int seismo,
+                           int psv, int sh, int acoustic, int slot, int l) {
     const int *pos = rec.pos + (long long)slot * 2 * rec.max_rec;
     const int i = pos[l], j = pos[rec.max_rec + l];
     const long long c = pidx(g, j, i);
@@ -748,6 +756,53 @@ __global__ void k_seismo(KGrid g, KState<T> S, KModel<T> M, KRec rec, int nt, in
         if (!acoustic) sec[3 * cs] = (float)(-fieldp(S, slot, P_SXX)[c] - fieldp(S, slot, P_SYY)[c]);
         else sec[3 * cs] = (float)(-fieldp(S, slot, P_SP)[c]);
     }
+}
+
+// After the stress update: the explosive sources and the free surface
+// (src/IFOS2D.c:1758-1768), one thread per column of row 1.  A column thread
+// first applies the sources located in its row-1 cell, in source order, then
+// the surface update of that cell; the thread of column 1 applies the sources
+// below row 1.  Every cell is thus changed by one thread, in the reference's
+// order.  grid: x over columns, y = slot.
+template <typename T, int FDOH>
+__global__ void k_surface_src(KGrid g, KState<T> S, KModel<T> M, KSrc src, int nt, int psv, int sh, int acoustic,
+                              int do_ps, int do_surf, KSnapPatch pt) {
+    pdl_wait();
+    pdl_launch();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int slot = blockIdx.y;
+    if (i > g.nx) return;
+    if (do_ps && psource_fires(src, slot)) {
+        const int n = src.nsrc[slot];
+        const float *pos = src.pos + (long long)slot * 8 * src.max_src;
+        for (int l = 0; l < n; l++) {
+            const int il = (int)pos[l], jl = (int)pos[src.max_src + l];
+            if (jl == 1 ? il == i : i == 1) psource_apply<T>(g, S, src, nt, acoustic, pt, slot, l);
+        }
+    }
+    if (do_surf) surface_cell<T, FDOH>(g, S, M, psv, sh, acoustic, pt, slot, i);
+}
+
+// the pressure residual at the receivers, ADJOINT_TYPE 4; grid: x over receivers, y = slot
+template <typename T>
+__global__ void k_psource_adj(KGrid g, KState<T> S, KRec rec, int nt, int acoustic) {
+    pdl_wait();
+    pdl_launch();
+    const int slot = blockIdx.y;
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < rec.ntr[slot]) psource_adj_rec<T>(g, S, rec, nt, acoustic, slot, l);
+}
+
+// receivers and the instability probe; grid: x over receivers, y = slot
+template <typename T, int FDOH>
+__global__ void k_seismo(KGrid g, KState<T> S, KModel<T> M, KRec rec, int nt, int seismo, int psv, int sh,
+                         int acoustic, int *bad) {
+    pdl_wait();
+    pdl_launch();
+    const int slot = blockIdx.y;
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l == 0) nan_probe<T>(g, S, psv, slot, bad);
+    if (seismo && l < rec.ntr[slot]) seismo_rec<T, FDOH>(g, S, M, rec, nt, seismo, psv, sh, acoustic, slot, l);
 }
 
 }  // namespace ifos

@@ -33,6 +33,8 @@ __device__ inline T snap_load(const KSnap &s, int slot, int snap, int k, long lo
 // fp32/fp64 snapshot copy (one thread per cell, all components)
 template <typename T>
 __global__ void k_snap_store(KGrid g, KState<T> S, KSnap sn, int hin) {
+    pdl_wait();
+    pdl_launch();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int slot = blockIdx.z;
@@ -45,6 +47,8 @@ __global__ void k_snap_store(KGrid g, KState<T> S, KSnap sn, int hin) {
 // low-precision snapshots, pass 1: absolute maximum of every component
 template <typename T>
 __global__ void k_snap_absmax(KGrid g, KState<T> S, KSnap sn, int hin) {
+    pdl_wait();
+    pdl_launch();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int slot = blockIdx.z;
@@ -62,6 +66,8 @@ __global__ void k_snap_absmax(KGrid g, KState<T> S, KSnap sn, int hin) {
 // low-precision snapshots, pass 2: scaled conversion (round to nearest even)
 template <typename T>
 __global__ void k_snap_quant(KGrid g, KState<T> S, KSnap sn, int hin) {
+    pdl_wait();
+    pdl_launch();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int slot = blockIdx.z;
@@ -88,6 +94,8 @@ struct KGrad {
 template <typename T>
 __global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad gr, int snap, int psv, int sh,
                             int acoustic) {
+    pdl_wait();
+    pdl_launch();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int slot = blockIdx.z;
@@ -127,9 +135,117 @@ __global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad g
     }
 }
 
+// Zero-lag correlation for fp32 state and fp32 snapshots: the arithmetic of
+// k_correlate per cell, two adjacent cells of a row per thread with 8-byte
+// loads and stores (rows of NX cells, NX even; the pitched state planes are
+// always pair-aligned).  Grid: x over pairs of a row, y = row, z = slot.
+struct CorrCell {
+    float vxp1, vyp1, sxx, syy, sxy, sp, vzp1, sxz, syz;  // adjoint state
+    float f[8];                                           // stored forward components
+};
+template <int PSV, int SH, int AC>
+__device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, float ll, float rho, float u, float *w0,
+                                               float *w1, float *w2, float *w3, float *w4) {
+    constexpr int KS = PSV ? (AC ? 3 : 5) : 0;  // first SH component
+    if (PSV) {
+        const float frx = a.f[0], fry = a.f[1];
+        *w2 += (float)((a.vxp1 * frx) + (a.vyp1 * fry));
+        if (!AC) {
+            const float fx = a.f[2], fy = a.f[3], fu = a.f[4];
+            *w0 += (float)((fx + fy) * (a.sxx + a.syy));
+            if (mm != 0.0f) {
+                const double t1 = (1.0 / (double)mm) * (double)(fu * a.sxy);
+                const double t2 = (.25 * (double)(fx + fy * (a.sxx + a.syy))) / (double)ll;
+                const double t3 = (.25 * (double)(fx - fy * (a.sxx - a.syy))) / (double)mm;
+                *w1 = (float)((double)*w1 + ((t1 + t2) + t3));
+            }
+        } else {
+            const float fp = a.f[2];
+            *w0 += (float)((fp) * (a.sp));
+        }
+    }
+    if (SH) {
+        const float frz = a.f[KS], fxz = a.f[KS + 1], fyz = a.f[KS + 2];
+        *w4 += (float)(a.vzp1 * frz);
+        const float muss = rho * u * u;
+        *w3 = (float)((double)*w3 + (1.0 / (double)(muss * muss)) * (double)(fxz * a.sxz + fyz * a.syz));
+    }
+}
+
+template <int PSV, int SH, int AC>
+__global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSnap sn, KGrad gr, int snap) {
+    pdl_wait();
+    pdl_launch();
+    constexpr int NC = (PSV ? (AC ? 3 : 5) : 0) + (SH ? 3 : 0);
+    // accumulators in use: lambda', mu', rho' (P-SV; acoustic: lambda', rho'), mu_z', rho_z' (SH)
+    constexpr bool use[5] = {PSV != 0, PSV && !AC, PSV != 0, SH != 0, SH != 0};
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
+    const int j = blockIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx) return;
+    const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1), n = gr.n;
+    const float *st = S.base + slot * S.slot_stride + c;
+    const float *fs = (const float *)((const char *)sn.base + slot * sn.slot_bytes + snap * sn.snap_bytes) + q;
+    float *acc = gr.acc + (long long)slot * 5 * n + q;
+    auto ld2 = [](const float *p) { return *reinterpret_cast<const float2 *>(p); };
+    CorrCell a0{}, a1{};
+    auto field = [&](int id, float &x0, float &x1) {
+        const float2 v = ld2(st + S.off[id]);
+        x0 = v.x;
+        x1 = v.y;
+    };
+    if (PSV) {
+        field(P_VXP1, a0.vxp1, a1.vxp1);
+        field(P_VYP1, a0.vyp1, a1.vyp1);
+        if (!AC) {
+            field(P_SXX, a0.sxx, a1.sxx);
+            field(P_SYY, a0.syy, a1.syy);
+            field(P_SXY, a0.sxy, a1.sxy);
+        } else {
+            field(P_SP, a0.sp, a1.sp);
+        }
+    }
+    if (SH) {
+        field(P_VZP1, a0.vzp1, a1.vzp1);
+        field(P_SXZ, a0.sxz, a1.sxz);
+        field(P_SYZ, a0.syz, a1.syz);
+    }
+#pragma unroll
+    for (int k = 0; k < NC; k++) {
+        const float2 v = ld2(fs + k * sn.n);
+        a0.f[k] = v.x;
+        a1.f[k] = v.y;
+    }
+    const long long mo = (long long)M.slot_model[slot] * M.model_stride + c;
+    float2 mm{0, 0}, ll{0, 0}, rho{0, 0}, u{0, 0};
+    if (PSV && !AC) {
+        mm = ld2(M.m[M_MM] + mo);
+        ll = ld2(M.m[M_LL] + mo);
+    }
+    if (SH) {
+        rho = ld2(M.m[M_RHO] + mo);
+        u = ld2(M.m[M_VS] + mo);
+    }
+    float2 w[5] = {};
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+        if (use[k]) w[k] = ld2(acc + k * n);
+    correlate_cell<PSV, SH, AC>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x);
+    const bool pair = i + 1 <= g.nx;
+    if (pair) correlate_cell<PSV, SH, AC>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y, &w[4].y);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        if (!use[k]) continue;
+        if (pair) *reinterpret_cast<float2 *>(acc + k * n) = w[k];
+        else acc[k * n] = w[k].x;
+    }
+}
+
 // per-shot gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2477-2601)
 template <typename T>
 __global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int acoustic) {
+    pdl_wait();
+    pdl_launch();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int slot = blockIdx.z;

@@ -6,9 +6,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "ifos_gpu.h"
@@ -30,6 +32,25 @@ static constexpr int kTileY = IFOS_TILE_Y;
 template <int FD, int NH, int NP, int NO>
 constexpr int ring_stages() {
     return Pipe<FD, kTileY, NH, NP, NO, 1>::bytes() * 6 + 2048 <= 232448 ? 3 : 2;
+}
+
+// Launch a kernel of the time loop as a programmatic dependent of the
+// preceding one (it starts while that one drains; its own griddepcontrol.wait
+// orders every dependent access).  Without IFOS_PDL (=0) a plain launch.
+template <typename... KArgs, typename... Args>
+static void launch_dep(cudaStream_t st, bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, args...);
 }
 // largest L on the pipelined path (more SLS fall back to one thread per cell)
 static constexpr int kPipeMaxL = 5;
@@ -86,6 +107,7 @@ struct ifos_ctx {
     // pipelined (TMA) stencil path: fp32, L <= kPipeMaxL
     bool pipe = false;
     bool fused_snap = false;  // fp32 snapshots written by the stencil kernels
+    bool pdl = true;          // time-loop kernels launched as programmatic dependents
     KMaps maps{};
     KTma ktma{};
     int num_sms = 148;
@@ -548,6 +570,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     c->slot_model_h.assign(S, 0);
     c->srcpos_h.assign((size_t)S * 8 * ms, 0.0f);
     setup_pipeline(c, L);
+    if (const char *e = std::getenv("IFOS_PDL")) c->pdl = std::atoi(e) != 0;
     CK(cudaStreamSynchronize(c->st));
     *out = c;
     return IFOS_OK;
@@ -790,7 +813,8 @@ struct Launcher {
         const long long ntiles =
             (long long)((c->p.nx + kTileX - 1) / kTileX) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
         const int grid = (int)std::min<long long>(ntiles, (long long)occ[d] * c->num_sms);
-        kern<<<grid, dim3(32, kComputeWarps + 1), P::bytes(), c->st>>>(c->maps, op, nshots, (int *)c->bad.p);
+        launch_dep(c->st, c->pdl, kern, dim3(grid), dim3(32, kComputeWarps + 1), P::bytes(), c->maps, op, nshots,
+                   (int *)c->bad.p);
     }
     // the snapshot a launch stores (hin < 0: none)
     KSnapOut snap_out(int hin) const {
@@ -928,18 +952,34 @@ struct Launcher {
         });
         c->launches += (c->ac ? 1 : c->psv + c->sh);
     }
-    void surface(const KSnapPatch &pt) {
+    // the explosive sources, free surface and receivers of a forward step
+    void post_fwd(int nt, bool psource, const KSnapPatch &pt) {
         const KGrid &g = c->g;
-        dim3 gs((c->p.nx + 127) / 128, nshots);
-        DISPATCH_FDOH(g.fdoh, k_surface<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, c->psv, c->sh, c->ac, pt));
+        if (psource || c->p.free_surf) {
+            const dim3 gs((unsigned)((c->p.nx + 127) / 128), (unsigned)nshots);
+            DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_surface_src<T, FD>, gs, dim3(128), 0, g, S, M, src, nt,
+                                             c->psv, c->sh, c->ac, psource ? 1 : 0, c->p.free_surf ? 1 : 0, pt));
+            c->launches++;
+        }
+        const dim3 gr((unsigned)((std::max(1, c->p.max_rec) + 127) / 128), (unsigned)nshots);
+        DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_seismo<T, FD>, gr, dim3(128), 0, g, S, M, rec, nt,
+                                         c->p.seismo, c->psv, c->sh, c->ac, (int *)c->bad.p));
         c->launches++;
     }
-    void seismo(int nt) {
+    // the residual pressure source and free surface of an adjoint step
+    void post_adj(int nt, bool psource) {
         const KGrid &g = c->g;
-        dim3 gs((std::max(1, c->p.max_rec) + 127) / 128, nshots);
-        DISPATCH_FDOH(g.fdoh, k_seismo<T, FD><<<gs, 128, 0, c->st>>>(g, S, M, rec, nt, c->p.seismo, c->psv, c->sh,
-                                                                     c->ac, (int *)c->bad.p));
-        c->launches++;
+        if (psource) {
+            const dim3 gr((unsigned)((std::max(1, c->p.max_rec) + 127) / 128), (unsigned)nshots);
+            launch_dep(c->st, c->pdl, k_psource_adj<T>, gr, dim3(128), 0, g, S, rec, nt, c->ac);
+            c->launches++;
+        }
+        if (c->p.free_surf) {
+            const dim3 gs((unsigned)((c->p.nx + 127) / 128), (unsigned)nshots);
+            DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_surface_src<T, FD>, gs, dim3(128), 0, g, S, M, src, nt,
+                                             c->psv, c->sh, c->ac, 0, 1, KSnapPatch{}));
+            c->launches++;
+        }
     }
 };
 
@@ -1008,7 +1048,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
             Lr.v_step(0, snap_now ? 1 : 0, fhin);
         }
         if (force) {
-            k_inject_v_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
+            launch_dep(c->st, c->pdl, k_inject_v_fwd<T>, dim3(nshots), dim3(32), 0, c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
                                                         c->sh);
             c->launches++;
         }
@@ -1016,22 +1056,17 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
             KTimer t(c, 1, sample);
             Lr.s_step(fhin);
         }
-        if (c->psv) {
-            k_psource_fwd<T><<<nshots, 32, 0, c->st>>>(c->g, Lr.S, Lr.src, nt, c->ac, pt);
-            c->launches++;
-        }
-        if (p.free_surf) Lr.surface(pt);
-        Lr.seismo(nt);
+        Lr.post_fwd(nt, c->psv != 0, pt);
         if (snap_now && fused) {
             hin++;
         } else if (snap_now) {
             KTimer t(c, 2, sample);
             if (p.snap_format == 0) {
-                k_snap_store<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
+                launch_dep(c->st, c->pdl, k_snap_store<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.S, sn, hin);
                 c->launches++;
             } else {
-                k_snap_absmax<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
-                k_snap_quant<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, sn, hin);
+                launch_dep(c->st, c->pdl, k_snap_absmax<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.S, sn, hin);
+                launch_dep(c->st, c->pdl, k_snap_quant<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.S, sn, hin);
                 c->launches += 2;
             }
             hin++;
@@ -1073,27 +1108,37 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
             Lr.v_step(1, 0);
         }
         if ((c->psv && p.adjoint_type >= 1 && p.adjoint_type <= 3) || c->sh) {
-            k_inject_v_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->psv ? 1 : 0, c->sh && !c->ac);
+            launch_dep(c->st, c->pdl, k_inject_v_adj<T>, dim3(gr_rec), dim3(128), 0, c->g, Lr.S, Lr.rec, nt, c->psv ? 1 : 0, c->sh && !c->ac);
             c->launches++;
         }
         {
             KTimer t(c, 1, sample);
             Lr.s_step();
         }
-        if (p.adjoint_type == 4) {
-            k_psource_adj<T><<<gr_rec, 128, 0, c->st>>>(c->g, Lr.S, Lr.rec, nt, c->ac);
-            c->launches++;
-        }
-        if (p.free_surf) Lr.surface(KSnapPatch{});
+        Lr.post_adj(nt, p.adjoint_type == 4);
         const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
         if ((fstep - 1) % p.dtinv == 0) {
             KTimer t(c, 3, sample);
-            k_correlate<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.S, Lr.M, sn, gr, ntd - hin_a, c->psv, c->sh, c->ac);
+            bool pairs = false;
+            if constexpr (std::is_same<T, float>::value) {
+                if (p.snap_format == 0 && p.nx % 2 == 0) {
+                    const dim3 gc((unsigned)((p.nx / 2 + 127) / 128), (unsigned)p.ny, (unsigned)nshots);
+                    const int h = ntd - hin_a;
+                    if (c->ac) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 0, 1>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    else if (c->psv && c->sh) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 1, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    else if (c->psv) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 0, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    else launch_dep(c->st, c->pdl, k_correlate_pairs<0, 1, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    pairs = true;
+                }
+            }
+            if (!pairs)
+                launch_dep(c->st, c->pdl, k_correlate<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.S, Lr.M, sn, gr, ntd - hin_a, c->psv, c->sh,
+                                                            c->ac);
             c->launches++;
             hin_a++;
         }
     }
-    k_assemble<T><<<Lr.grd, Lr.blk, 0, c->st>>>(c->g, Lr.M, gr, c->psv, c->sh, c->ac);
+    launch_dep(c->st, c->pdl, k_assemble<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.M, gr, c->psv, c->sh, c->ac);
     c->launches++;
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaGetLastError());

@@ -153,33 +153,53 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
     __syncthreads();
     if (warp == kComputeWarps) {
         if (threadIdx.x != 0) return;
-        for (int k = 0;; k++) {
-            const int t = blockIdx.x + k * gridDim.x;
-            if (t >= ntiles) break;
+        // Tile k in stage k % NST.  The per-cell planes of the first NST tiles
+        // are not written by the preceding kernel of the stream, so they are
+        // requested before waiting for it; everything else after.
+        auto issue = [&](int k, bool halo, bool plain) {
             const int st = k % NST;
-            if (k >= NST && !mbar_wait_bounded(&empty[st], (uint32_t)(((k / NST) - 1) & 1), err, 18)) {
-                abort_flag = 1;
-                break;
-            }
             TileInfo ti;
-            tile_of(t, ntx, nty, TY, ti);
-            ti.model = op.M.slot_model[ti.slot];
-            ti.ystrip = tile_in_ystrip(g, ti.j0, TY);
-            tinfo[st] = ti;
+            tile_of(blockIdx.x + k * gridDim.x, ntx, nty, TY, ti);
             float *stage = smem + st * P::STAGE;
             uint64_t *bar = &full[st];
+            if (plain) {
+                ti.model = op.M.slot_model[ti.slot];
+                ti.ystrip = tile_in_ystrip(g, ti.j0, TY);
+                tinfo[st] = ti;
+                mbar_expect_tx(bar, P::TXB);
+            } else {
+                ti.model = tinfo[st].model;
+            }
             int hz[NH > 0 ? NH : 1];
             PlainSrc pz[NP > 0 ? NP : 1];
             op.planes(ti, hz, pz);
-            const int bx = HX + ti.i0 - 1 - P::XH, by = HY + ti.j0 - 1 - P::H;
-            const int px = HX + ti.i0 - 1, py = HY + ti.j0 - 1;
-            mbar_expect_tx(bar, P::TXB);
+            if (halo) {
+                const int bx = HX + ti.i0 - 1 - P::XH, by = HY + ti.j0 - 1 - P::H;
 #pragma unroll
-            for (int h = 0; h < NH; h++) tma_load_3d(stage + h * P::BOXS, &mp.halo, bx, by, hz[h], bar);
+                for (int h = 0; h < NH; h++) tma_load_3d(stage + h * P::BOXS, &mp.halo, bx, by, hz[h], bar);
+            }
+            if (plain) {
+                const int px = HX + ti.i0 - 1, py = HY + ti.j0 - 1;
 #pragma unroll
-            for (int q = 0; q < NP; q++)
-                tma_load_3d(stage + NH * P::BOXS + q * P::PLS, pz[q].model ? &mp.model : &mp.plain, px, py, pz[q].z,
-                            bar);
+                for (int q = 0; q < NP; q++)
+                    tma_load_3d(stage + NH * P::BOXS + q * P::PLS, pz[q].model ? &mp.model : &mp.plain, px, py,
+                                pz[q].z, bar);
+            }
+        };
+        int npre = 0;
+        while (npre < NST && blockIdx.x + npre * gridDim.x < ntiles) issue(npre++, false, true);
+        pdl_wait();
+        for (int k = 0; k < npre; k++) issue(k, true, false);
+        pdl_launch();
+        for (int k = npre;; k++) {
+            const int t = blockIdx.x + k * gridDim.x;
+            if (t >= ntiles) break;
+            const int st = k % NST;
+            if (!mbar_wait_bounded(&empty[st], (uint32_t)(((k / NST) - 1) & 1), err, 18)) {
+                abort_flag = 1;
+                break;
+            }
+            issue(k, true, true);
         }
         return;
     }
