@@ -27,11 +27,18 @@ using namespace ifos;
 #endif
 static constexpr int kTileY = IFOS_TILE_Y;
 
-// Stages of an op's shared-memory ring: three when two blocks of three fit
-// in an SM's 227 KB, else two (the ring then still holds two blocks).
+// Stages of an op's shared-memory ring: as many as fit when kRingBlocks
+// blocks share an SM's 227 KB (2..6).  Loads stay in flight in every stage
+// but the one being computed, so deeper rings keep more bytes in flight.
+#ifndef IFOS_RING_BLOCKS
+#define IFOS_RING_BLOCKS 3
+#endif
+constexpr int kRingBlocks = IFOS_RING_BLOCKS;
 template <int FD, int NH, int NP, int NO>
 constexpr int ring_stages() {
-    return Pipe<FD, kTileY, NH, NP, NO, 1>::bytes() * 6 + 2048 <= 232448 ? 3 : 2;
+    constexpr size_t stage = Pipe<FD, kTileY, NH, NP, NO, 1>::bytes();
+    constexpr int n = (int)((232448 / kRingBlocks - 1024) / stage);
+    return n < 2 ? 2 : (n > 6 ? 6 : n);
 }
 
 // Launch a kernel of the time loop as a programmatic dependent of the
