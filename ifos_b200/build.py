@@ -17,6 +17,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifos_b200.so")
 SOURCES = ["ifos_solver.cu", "ifos_setup.cpp", "ifos_noalloc.cu"]
+# the reference-named per-kernel entry points; the driver defines the globals they read
+LIB_COMPAT = os.path.join(HERE, "libifos_compat.so")
+SOURCES_COMPAT = ["ifos_compat.cu"]
 HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h", "ifos_tma.cuh", "ifos_tile.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -28,29 +31,36 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libifos_b200.so")
 
 
-def _inputs():
-    files = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
-    files.append(os.path.join(ROOT, "include", "ifos_gpu.h"))
+def _inputs(sources, header):
+    files = [os.path.join(CSRC, s) for s in sources + HEADERS]
+    files.append(os.path.join(ROOT, "include", header))
     return files
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+def up_to_date(lib=LIB, sources=SOURCES, header="ifos_gpu.h") -> bool:
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in _inputs())
+    t = os.path.getmtime(lib)
+    return all(os.path.getmtime(f) <= t for f in _inputs(sources, header))
 
 
-def build(force: bool = False, verbose: bool = False, extra=()) -> str:
-    if not force and up_to_date():
-        return LIB
+def _compile(lib, sources, verbose, extra):
     cmd = [nvcc(), "-O3", *ARCH, "-lineinfo", "--fmad=false", "-std=c++17", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart", *extra]
+           "-o", lib + ".tmp", *[os.path.join(CSRC, s) for s in sources], "-lcudart", *extra]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
+    os.replace(lib + ".tmp", lib)
+
+
+def build(force: bool = False, verbose: bool = False, extra=()) -> str:
+    """Build libifos_b200.so (the shot solver) and libifos_compat.so (the
+    reference-named per-kernel entry points); returns the solver library."""
+    if force or not up_to_date():
+        _compile(LIB, SOURCES, verbose, extra)
+    if force or not up_to_date(LIB_COMPAT, SOURCES_COMPAT, "ifos_compat.h"):
+        _compile(LIB_COMPAT, SOURCES_COMPAT, verbose, extra)
     return LIB
 
 
