@@ -366,4 +366,85 @@ __global__ void k_calc_res(const float *obs, const float *syn, float *diff, int 
     en_tr[tr] = en;
 }
 
+// Offset-based trace kill (src/create_trkill_table.c:35-46): killtable[r][s]
+// is set to 1 where the source-receiver offset, formed in float and taken
+// through a double sqrt as the reference does, lies strictly inside
+// (lower, upper); other entries are left as they are.  One thread per pair.
+__global__ void k_trkill(int ntr, const int *rx, const int *ry, int nsrc, const float *sx, const float *sy, float dh,
+                         float lower, float upper, int *killtable) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= (long long)ntr * nsrc) return;
+    const int r = (int)(k / nsrc), s = (int)(k % nsrc);
+    const float ddx = sx[s] - rx[r] * dh, ddy = sy[s] - ry[r] * dh;
+    const float offset = (float)fabs(sqrt((double)(ddx * ddx + ddy * ddy)));
+    if (offset > lower && offset < upper) killtable[k] = 1;
+}
+
+// Time windows around picked first arrivals (src/time_window.c:146-220),
+// one thread per sample j = 2..ns of a trace; tw_ind 0: one pick per trace
+// with lengths twl_plus/twl_minus; 1: (pick, length+, length-); 2: two such
+// windows, the first one's tapered copy added to the second's.  mask (if
+// not NULL) records the tapers applied: bits 0/1 the first window's late/early
+// taper, bits 2/3 the second window's.
+__global__ void k_time_window(float *sec, int ntr, int ns, int tw_ind, const float *picks, float dt, float gamma,
+                              float twl_plus, float twl_minus, unsigned char *mask) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= (long long)ntr * ns) return;
+    const int i = (int)(k / ns), j = (int)(k % ns) + 1;  // trace, 1-based sample
+    if (j < 2) return;
+    const float time = (float)(j * dt);
+    float v = sec[k];
+    unsigned char m = 0;
+    float p1, l1, l2;
+    if (tw_ind == 1 || tw_ind == 2) {
+        p1 = picks[i];
+        l1 = picks[ntr + i];
+        l2 = picks[2 * ntr + i];
+    } else {
+        p1 = picks[i];
+        l1 = twl_plus;
+        l2 = twl_minus;
+    }
+    const float dumpa = (time - p1 - l1);
+    const float taper = (float)exp((double)(-gamma * dumpa));
+    const float dumpb = (time - p1 + l2);
+    const float taper1 = (float)exp((double)(-gamma * dumpb));
+    if (tw_ind != 2) {
+        if (time >= p1 + l1) {
+            v = v * taper;
+            m |= 1;
+        }
+        if (time <= p1 - l2) {
+            v = v * taper1;
+            m |= 2;
+        }
+    } else {
+        float dummy = v;
+        if (time >= p1 + l1) {
+            dummy = v * taper;
+            m |= 1;
+        }
+        if (time <= p1 - l2) {
+            dummy = v * taper1;
+            m |= 2;
+        }
+        const float p4 = picks[3 * ntr + i], l5 = picks[4 * ntr + i], l6 = picks[5 * ntr + i];
+        const float dumpc = (time - p4 - l5);
+        const float taper2 = (float)exp((double)(-gamma * dumpc));
+        const float dumpd = (time - p4 + l6);
+        const float taper3 = (float)exp((double)(-gamma * dumpd));
+        if (time >= p4 + l5) {
+            v = v * taper2;
+            m |= 4;
+        }
+        if (time <= p4 - l6) {
+            v = v * taper3;
+            m |= 8;
+        }
+        v = v + dummy;
+    }
+    sec[k] = v;
+    if (mask) mask[k] = m;
+}
+
 }  // namespace ifos

@@ -1358,6 +1358,75 @@ extern "C" int ifos_sync(ifos_ctx *c) {
     return IFOS_OK;
 }
 
+extern "C" int ifos_trkill_table(ifos_ctx *c, int ntr, const int *rx, const int *ry, int nsrc, const float *sx,
+                                 const float *sy, float lower, float upper, int *killtable) {
+    if (!c) return IFOS_ERR_ARG;
+    if (ntr < 0 || nsrc < 0 || (ntr && (!rx || !ry)) || (nsrc && (!sx || !sy)) || (ntr && nsrc && !killtable))
+        return fail(c, IFOS_ERR_ARG, "bad trace-kill arguments");
+    if (!ntr || !nsrc) return IFOS_OK;
+    CK(cudaSetDevice(c->device));
+    DevBuf b_rx, b_ry, b_sx, b_sy, b_k;
+    const size_t nk = (size_t)ntr * nsrc;
+    int rc = IFOS_OK;
+    if ((rc = dev_alloc(c, b_rx, ntr * sizeof(int))) || (rc = dev_alloc(c, b_ry, ntr * sizeof(int))) ||
+        (rc = dev_alloc(c, b_sx, nsrc * sizeof(float))) || (rc = dev_alloc(c, b_sy, nsrc * sizeof(float))) ||
+        (rc = dev_alloc(c, b_k, nk * sizeof(int)))) {
+        dev_free(b_rx), dev_free(b_ry), dev_free(b_sx), dev_free(b_sy), dev_free(b_k);
+        return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(b_rx.p, rx, ntr * sizeof(int), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b_ry.p, ry, ntr * sizeof(int), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b_sx.p, sx, nsrc * sizeof(float), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b_sy.p, sy, nsrc * sizeof(float), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b_k.p, killtable, nk * sizeof(int), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        k_trkill<<<(unsigned)((nk + 255) / 256), 256, 0, c->st>>>(ntr, (const int *)b_rx.p, (const int *)b_ry.p, nsrc,
+                                                                  (const float *)b_sx.p, (const float *)b_sy.p,
+                                                                  c->p.dh, lower, upper, (int *)b_k.p);
+        c->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(killtable, b_k.p, nk * sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    dev_free(b_rx), dev_free(b_ry), dev_free(b_sx), dev_free(b_sy), dev_free(b_k);
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, std::string("ifos_trkill_table: ") + cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_time_window(ifos_ctx *c, int ntr, int ns, float *sections, int tw_ind, const float *picks,
+                                float gamma, float twl_plus, float twl_minus, unsigned char *mask) {
+    if (!c) return IFOS_ERR_ARG;
+    if (ntr < 0 || ns < 0 || tw_ind < 0 || tw_ind > 2 || (ntr && ns && (!sections || !picks)))
+        return fail(c, IFOS_ERR_ARG, "bad time-window arguments");
+    if (!ntr || !ns) return IFOS_OK;
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)ntr * ns;
+    const int np = tw_ind == 1 ? 3 : (tw_ind == 2 ? 6 : 1);
+    DevBuf b_s, b_p, b_m;
+    int rc = IFOS_OK;
+    if ((rc = dev_alloc(c, b_s, n * sizeof(float))) || (rc = dev_alloc(c, b_p, (size_t)np * ntr * sizeof(float))) ||
+        (mask && (rc = dev_alloc(c, b_m, n)))) {
+        dev_free(b_s), dev_free(b_p), dev_free(b_m);
+        return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(b_s.p, sections, n * sizeof(float), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b_p.p, picks, (size_t)np * ntr * sizeof(float), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        k_time_window<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>((float *)b_s.p, ntr, ns, tw_ind,
+                                                                      (const float *)b_p.p, c->p.dt, gamma, twl_plus,
+                                                                      twl_minus, (unsigned char *)b_m.p);
+        c->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sections, b_s.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess && mask) e = cudaMemcpyAsync(mask, b_m.p, n, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    dev_free(b_s), dev_free(b_p), dev_free(b_m);
+    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, std::string("ifos_time_window: ") + cudaGetErrorString(e));
+    return IFOS_OK;
+}
+
 extern "C" int ifos_fd_coeffs(const ifos_params *p, float *hc7) {
     if (!p || !hc7) return IFOS_ERR_ARG;
     return fd_coefficients(p->fdorder, p->maxrelerror, hc7) ? IFOS_OK : IFOS_ERR_ARG;

@@ -170,6 +170,32 @@ class ShotSolver:
                                            C.byref(en)))
         return diff, l2.value, en.value
 
+    def trkill_table(self, rec_xy, src_xy, lower, upper, table=None):
+        """Offset-based trace-kill table (src/create_trkill_table.c): rec_xy
+        (2, ntr) receiver grid indices, src_xy (2, nsrc) source coordinates in
+        metres; returns the (ntr, nsrc) int table with 1 where killed (entries
+        of `table` kept otherwise)."""
+        rx, ry = (np.ascontiguousarray(a, np.int32) for a in np.asarray(rec_xy))
+        sx, sy = (np.ascontiguousarray(a, np.float32) for a in np.asarray(src_xy, np.float32))
+        k = (np.zeros((rx.size, sx.size), np.int32) if table is None else np.ascontiguousarray(table, np.int32).copy())
+        IP = C.POINTER(C.c_int)
+        self._check(self.lib.ifos_trkill_table(self._ctx, rx.size, rx.ctypes.data_as(IP), ry.ctypes.data_as(IP),
+                                               sx.size, _fp(sx), _fp(sy), float(lower), float(upper),
+                                               k.ctypes.data_as(IP)))
+        return k
+
+    def time_window(self, sections, tw_ind, picks, gamma, twl_plus=0.0, twl_minus=0.0, want_mask=False):
+        """Time windows around first-arrival picks (src/time_window.c) on a
+        (ntr, ns) section; picks (ntr,), (3, ntr) or (6, ntr) for tw_ind 0/1/2.
+        Returns the windowed section (and the per-sample taper mask)."""
+        sec = _f32(sections).copy()
+        pk = _f32(picks)
+        mask = np.zeros(sec.shape, np.uint8) if want_mask else None
+        self._check(self.lib.ifos_time_window(self._ctx, sec.shape[0], sec.shape[1], _fp(sec), int(tw_ind), _fp(pk),
+                                              float(gamma), float(twl_plus), float(twl_minus),
+                                              mask.ctypes.data_as(C.POINTER(C.c_ubyte)) if want_mask else None))
+        return (sec, mask) if want_mask else sec
+
     def grad_sum_device(self, nshots, dev_ptr: int):
         """Write the summed gradients (5 x NY x NX float32) to device memory."""
         self._check(self.lib.ifos_grad_sum_device(self._ctx, int(nshots), C.c_void_p(dev_ptr)))

@@ -164,6 +164,28 @@ int ifos_dot_f64(ifos_ctx *ctx, const float *a, const float *b, size_t n, int de
 int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, float *diff, double *l2,
                   double *energy);
 
+/* Offset-based trace-kill table (src/create_trkill_table.c:21-46), on the
+ * device and bit-identical to the reference: killtable (ntr_glob x nsrc_glob,
+ * row-major [receiver][source], host, in/out) gets 1 where the offset between
+ * source s at (sx[s], sy[s]) metres and receiver r at grid point
+ * (rx[r], ry[r]) (times DH) lies strictly between lower and upper; other
+ * entries keep their values (the driver zeroes the table first or adds the
+ * offset kill to a table read from file). */
+int ifos_trkill_table(ifos_ctx *ctx, int ntr_glob, const int *rx, const int *ry, int nsrc_glob, const float *sx,
+                      const float *sy, float lower, float upper, int *killtable);
+
+/* Time windows around picked first arrivals (src/time_window.c:24-224) on
+ * ntr traces of ns samples (host, row-major, in/out), samples 2..ns as the
+ * reference: tw_ind 0 takes picks[ntr] with twl_plus/twl_minus, 1 takes
+ * picks[3][ntr] (pick, length+, length-), 2 takes picks[6][ntr] (two windows).
+ * The picks are those of the local traces (the reference's recpos_loc[3]
+ * mapping is the caller's).  mask (NULL or ntr x ns) receives per sample the
+ * tapers applied (bits 0/1: late/early taper of the first window, 2/3: of the
+ * second).  The sample selection is bit-identical to the reference; the taper
+ * values use the device's exp(). */
+int ifos_time_window(ifos_ctx *ctx, int ntr, int ns, float *sections, int tw_ind, const float *picks, float gamma,
+                     float twl_plus, float twl_minus, unsigned char *mask);
+
 /* Host-only set-up queries (no device needed): the FD weights hc[0..6]
  * (src/holbergcoeff.c:37-108) and the CPML profiles as 12 arrays of 2*FW+1
  * floats, 1-based, in the order K_x a_x b_x K_x_half a_x_half b_x_half K_y a_y
