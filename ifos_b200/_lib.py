@@ -24,8 +24,10 @@ EXPORTS = [
     "ifos_fetch_sections", "ifos_fetch_grads", "ifos_grad_sum", "ifos_forward_steps", "ifos_fetch_fields",
     "ifos_dot_f64", "ifos_calc_res", "ifos_fd_coeffs", "ifos_cpml_profiles", "ifos_kernel_timing",
     "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_dot_f64_noalloc", "ifos_last_ms", "ifos_launch_count",
-    "ifos_sync", "ifos_trkill_table", "ifos_time_window",
+    "ifos_sync", "ifos_trkill_table", "ifos_time_window", "ifos_set_option", "ifos_get_option",
+    "ifos_residual_adjoint",
 ]
+OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3}
 
 
 class IfosParams(C.Structure):
@@ -100,6 +102,9 @@ def load():
         "ifos_trkill_table": (C.c_int, [vp, C.c_int, IP, IP, C.c_int, FP, FP, C.c_float, C.c_float, IP]),
         "ifos_time_window": (C.c_int, [vp, C.c_int, C.c_int, FP, C.c_int, FP, C.c_float, C.c_float, C.c_float,
                                        C.POINTER(C.c_ubyte)]),
+        "ifos_set_option": (C.c_int, [vp, C.c_int, C.c_int]),
+        "ifos_get_option": (C.c_int, [vp, C.c_int, IP]),
+        "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, DP, DP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -51,6 +51,7 @@ struct KGrid {
     int k_one;       // every CPML K profile value is 1: d/K == d exactly
     int dh_pow2;     // DH is a power of two: x/DH == x*inv_dh exactly
     float inv_dh;    // 1/DH (exact when dh_pow2)
+    int tile_order;  // pipelined stencils: 0 slot-major tile sequence, 1 slot-minor
 };
 
 // x / DH, exact in both branches: multiplying by the reciprocal of a power of

@@ -391,7 +391,10 @@ __global__ void k_time_window(float *sec, int ntr, int ns, int tw_ind, const flo
     const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= (long long)ntr * ns) return;
     const int i = (int)(k / ns), j = (int)(k % ns) + 1;  // trace, 1-based sample
-    if (j < 2) return;
+    if (j < 2) {  // the reference's loops start at sample 2
+        if (mask) mask[k] = 0;
+        return;
+    }
     const float time = (float)(j * dt);
     float v = sec[k];
     unsigned char m = 0;

@@ -71,6 +71,21 @@ struct DevBuf {
 };
 }  // namespace
 
+// a sampled kernel-class interval (start and end event)
+struct TimedPair {
+    int cls;
+    cudaEvent_t e0, e1;
+};
+// one captured time loop: the instantiated graph, the launch sequence it was
+// captured for (key), the kernels it launches, and its timing events
+struct LoopGraph {
+    std::string key;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+    std::vector<cudaEvent_t> events;
+    std::vector<TimedPair> pairs;
+};
+
 struct ifos_ctx {
     ifos_params p{};
     int device = 0;
@@ -108,7 +123,7 @@ struct ifos_ctx {
     int prof_stride = 0;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
-    std::vector<std::pair<int, size_t>> ev_pairs;  // (class, index of start event)
+    std::vector<TimedPair> ev_pairs;
     double kt_ms[4] = {0, 0, 0, 0};
     long long kt_n[4] = {0, 0, 0, 0};
     // pipelined (TMA) stencil path: fp32, L <= kPipeMaxL
@@ -118,9 +133,15 @@ struct ifos_ctx {
     KMaps maps{};
     KTma ktma{};
     int num_sms = 148;
+    // execution options (IFOS_OPT_*)
+    bool graphs = true;     // time loops captured once and replayed as CUDA graphs
+    int blocks_per_sm = 0;  // persistent stencil CTAs per SM (0: as many as fit)
+    cudaStream_t cap_st = nullptr;  // capture stream (the caller's may be the legacy default stream)
+    LoopGraph gfwd, gadj;
 };
 
-// Events for the sampled kernel timing come from a pool that grows on demand.
+// Events for the sampled kernel timing come from a pool that grows on demand;
+// a captured loop takes the events it recorded out of the pool and owns them.
 static cudaEvent_t pool_event(ifos_ctx *c) {
     if (c->ev_used == c->ev_pool.size()) {
         cudaEvent_t e;
@@ -132,36 +153,35 @@ static cudaEvent_t pool_event(ifos_ctx *c) {
 struct KTimer {
     ifos_ctx *c;
     int cls;
-    size_t idx = 0;
-    bool on;
-    KTimer(ifos_ctx *cc, int k, bool sample) : c(cc), cls(k), on(sample && cc->prof_stride > 0) {
-        if (!on) return;
-        idx = c->ev_used;
-        cudaEvent_t e = pool_event(c);
-        if (!e) {
-            on = false;
-            return;
-        }
-        cudaEventRecord(e, c->st);
+    cudaEvent_t e0 = nullptr;
+    KTimer(ifos_ctx *cc, int k, bool sample) : c(cc), cls(k) {
+        if (!(sample && cc->prof_stride > 0)) return;
+        e0 = pool_event(c);
+        if (e0) cudaEventRecord(e0, c->st);
     }
     ~KTimer() {
-        if (!on) return;
-        cudaEvent_t e = pool_event(c);
-        if (!e) return;
-        cudaEventRecord(e, c->st);
-        c->ev_pairs.push_back({cls, idx});
+        if (!e0) return;
+        cudaEvent_t e1 = pool_event(c);
+        if (!e1) return;
+        cudaEventRecord(e1, c->st);
+        c->ev_pairs.push_back({cls, e0, e1});
     }
 };
 static void collect_kernel_times(ifos_ctx *c) {
     for (auto &pr : c->ev_pairs) {
         float ms = 0.0f;
-        if (cudaEventElapsedTime(&ms, c->ev_pool[pr.second], c->ev_pool[pr.second + 1]) == cudaSuccess) {
-            c->kt_ms[pr.first] += ms;
-            c->kt_n[pr.first]++;
+        if (cudaEventElapsedTime(&ms, pr.e0, pr.e1) == cudaSuccess) {
+            c->kt_ms[pr.cls] += ms;
+            c->kt_n[pr.cls]++;
         }
     }
     c->ev_pairs.clear();
     c->ev_used = 0;
+}
+static void drop_graph(LoopGraph &lg) {
+    if (lg.exec) cudaGraphExecDestroy(lg.exec);
+    for (cudaEvent_t e : lg.events) cudaEventDestroy(e);
+    lg = LoopGraph{};
 }
 
 // ----------------------------------------------------------------------------
@@ -194,6 +214,18 @@ static void dev_free(DevBuf &b) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
+}
+
+// Grow-only per-context scratch (the res_tr buffer): a call that needs no more
+// than any call before it allocates nothing, so concurrent contexts on other
+// streams are not stalled by the device-wide synchronisation of cudaFree.
+static int scratch(ifos_ctx *c, size_t bytes, void **out) {
+    if (c->res_tr.bytes < bytes) {
+        CK(cudaStreamSynchronize(c->st));
+        if (int rc = dev_alloc(c, c->res_tr, bytes)) return rc;
+    }
+    *out = c->res_tr.p;
+    return IFOS_OK;
 }
 
 static int check_params(const ifos_params &p, std::string &why) {
@@ -310,6 +342,9 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
                       &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
     for (DevBuf *b : bufs) dev_free(*b);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    drop_graph(c->gfwd);
+    drop_graph(c->gadj);
+    if (c->cap_st) cudaStreamDestroy(c->cap_st);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_st) cudaStreamDestroy(c->own_st);
@@ -407,6 +442,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed"));
     if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cap_st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
         return bail(fail(c, IFOS_ERR_CUDA, "stream/event creation failed"));
     c->st = c->own_st;
@@ -578,6 +614,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     c->srcpos_h.assign((size_t)S * 8 * ms, 0.0f);
     setup_pipeline(c, L);
     if (const char *e = std::getenv("IFOS_PDL")) c->pdl = std::atoi(e) != 0;
+    if (const char *e = std::getenv("IFOS_GRAPHS")) c->graphs = std::atoi(e) != 0;
     CK(cudaStreamSynchronize(c->st));
     *out = c;
     return IFOS_OK;
@@ -819,7 +856,8 @@ struct Launcher {
         }
         const long long ntiles =
             (long long)((c->p.nx + kTileX - 1) / kTileX) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
-        const int grid = (int)std::min<long long>(ntiles, (long long)occ[d] * c->num_sms);
+        const int bps = c->blocks_per_sm > 0 ? std::min(c->blocks_per_sm, occ[d]) : occ[d];
+        const int grid = (int)std::min<long long>(ntiles, (long long)bps * c->num_sms);
         launch_dep(c->st, c->pdl, kern, dim3(grid), dim3(32, kComputeWarps + 1), P::bytes(), c->maps, op, nshots,
                    (int *)c->bad.p);
     }
@@ -1014,6 +1052,65 @@ static int zero_state(ifos_ctx *c, int nshots) {
     return IFOS_OK;
 }
 
+// Run one time loop; enqueue() issues its launches on c->st.  With graphs
+// on, the loop is captured once per launch sequence (key) on the capture
+// stream and the instantiated graph is replayed on c->st by every later call
+// with the same key: every per-shot input the kernels read (sources,
+// receivers, adjoint sources, model index) lives in device buffers that
+// ifos_shot_setup / ifos_stage_adjoint rewrite in place.
+template <typename F>
+static int run_loop(ifos_ctx *c, LoopGraph &lg, const std::string &key, F &&enqueue) {
+    if (!c->graphs) {
+        enqueue();
+        CK(cudaGetLastError());
+        return IFOS_OK;
+    }
+    if (lg.key != key || !lg.exec) {
+        drop_graph(lg);
+        cudaStream_t user = c->st;
+        const long long l0 = c->launches;
+        const size_t e_first = c->ev_used, p_first = c->ev_pairs.size();
+        c->st = c->cap_st;
+        cudaError_t e = cudaStreamBeginCapture(c->cap_st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue();
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(c->cap_st, &g);
+            if (e == cudaSuccess) {
+                e = cudaGraphInstantiate(&lg.exec, g, 0);
+                cudaGraphDestroy(g);
+            }
+        }
+        c->st = user;
+        lg.launches = c->launches - l0;
+        c->launches = l0;
+        // the graph owns the timing events it records
+        lg.events.assign(c->ev_pool.begin() + e_first, c->ev_pool.begin() + c->ev_used);
+        c->ev_pool.erase(c->ev_pool.begin() + e_first, c->ev_pool.begin() + c->ev_used);
+        c->ev_used = e_first;
+        lg.pairs.assign(c->ev_pairs.begin() + p_first, c->ev_pairs.end());
+        c->ev_pairs.resize(p_first);
+        if (e != cudaSuccess) {
+            drop_graph(lg);
+            cudaGetLastError();
+            return fail(c, IFOS_ERR_CUDA, std::string("time-loop graph capture: ") + cudaGetErrorString(e));
+        }
+        lg.key = key;
+    }
+    CK(cudaGraphLaunch(lg.exec, c->st));
+    c->launches += lg.launches;
+    c->ev_pairs.insert(c->ev_pairs.end(), lg.pairs.begin(), lg.pairs.end());
+    return IFOS_OK;
+}
+
+static std::string loop_key(const ifos_ctx *c, std::initializer_list<long long> v) {
+    std::string k;
+    for (long long x : v) k += std::to_string(x) + ",";
+    k += std::to_string(c->prof_stride) + "," + std::to_string(c->pdl) + "," + std::to_string(c->blocks_per_sm) + "," +
+         std::to_string(c->g.tile_order);
+    return k;
+}
+
 template <typename T>
 static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     const ifos_params &p = c->p;
@@ -1044,6 +1141,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     pt.c_sp = comp_of(P_SP);
     pt.c_syz = comp_of(P_SYZ);
     CK(cudaEventRecord(c->ev0, c->st));
+    auto enqueue = [&]() {
     int hin = 0;
     for (int nt = 1; nt <= nsteps; nt++) {
         const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
@@ -1079,6 +1177,8 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
             hin++;
         }
     }
+    };
+    if (int rc = run_loop(c, c->gfwd, loop_key(c, {0, nshots, snaps, nsteps, force, fused}), enqueue)) return rc;
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));
@@ -1107,6 +1207,7 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     const int mr = std::max(1, p.max_rec);
     dim3 gr_rec((mr + 127) / 128, nshots);
     CK(cudaEventRecord(c->ev0, c->st));
+    auto enqueue = [&]() {
     int hin_a = 1;
     for (int nt = 1; nt <= p.nt; nt++) {
         const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
@@ -1147,6 +1248,8 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     }
     launch_dep(c->st, c->pdl, k_assemble<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.M, gr, c->psv, c->sh, c->ac);
     c->launches++;
+    };
+    if (int rc = run_loop(c, c->gadj, loop_key(c, {1, nshots}), enqueue)) return rc;
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));
@@ -1219,14 +1322,12 @@ extern "C" int ifos_grad_sum(ifos_ctx *c, int nshots, float *out) {
     if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
     CK(cudaSetDevice(c->device));
     const long long N = (long long)c->p.nx * c->p.ny;
-    DevBuf tmp;
-    if (int rc = dev_alloc(c, tmp, (size_t)5 * N * 4)) return rc;
-    k_grad_sum<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>((const float *)c->gout.p, nshots, N, (float *)tmp.p);
+    void *tmp = nullptr;
+    if (int rc = scratch(c, (size_t)5 * N * 4, &tmp)) return rc;
+    k_grad_sum<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>((const float *)c->gout.p, nshots, N, (float *)tmp);
     c->launches++;
-    cudaError_t e = cudaMemcpyAsync(out, tmp.p, (size_t)5 * N * 4, cudaMemcpyDeviceToHost, c->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-    dev_free(tmp);
-    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(out, tmp, (size_t)5 * N * 4, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     return IFOS_OK;
 }
 
@@ -1242,24 +1343,19 @@ __global__ void k_fields_out(KGrid g, KState<T> S, int slot, const int *ids, int
 template <typename T>
 static int fetch_fields_t(ifos_ctx *c, int slot, float *fields) {
     const long long N = (long long)c->p.nx * c->p.ny;
-    DevBuf tmp, ids;
-    if (int rc = dev_alloc(c, tmp, (size_t)IFOS_NF * N * 4)) return rc;
-    if (int rc = dev_alloc(c, ids, IFOS_NF * sizeof(int))) {
-        dev_free(tmp);
-        return rc;
-    }
+    void *tmp = nullptr;
+    const size_t fb = (size_t)IFOS_NF * N * 4;
+    if (int rc = scratch(c, fb + 256, &tmp)) return rc;
+    int *ids = (int *)((char *)tmp + fb);
     int idh[IFOS_NF];
     const int map[IFOS_NF] = {P_VX, P_VY, P_SXX, P_SYY, P_SXY, P_VXP1, P_VYP1, P_VZ, P_SXZ, P_SYZ, P_VZP1, P_SP};
     for (int k = 0; k < IFOS_NF; k++) idh[k] = c->off[map[k]] >= 0 ? map[k] : -1;
-    cudaMemcpyAsync(ids.p, idh, sizeof idh, cudaMemcpyHostToDevice, c->st);
+    CK(cudaMemcpyAsync(ids, idh, sizeof idh, cudaMemcpyHostToDevice, c->st));
     dim3 blk(32, 8), grd((c->p.nx + 31) / 32, (c->p.ny + 7) / 8);
-    k_fields_out<T><<<grd, blk, 0, c->st>>>(c->g, kstate<T>(c), slot, (const int *)ids.p, IFOS_NF, (float *)tmp.p);
+    k_fields_out<T><<<grd, blk, 0, c->st>>>(c->g, kstate<T>(c), slot, ids, IFOS_NF, (float *)tmp);
     c->launches++;
-    cudaError_t e = cudaMemcpyAsync(fields, tmp.p, (size_t)IFOS_NF * N * 4, cudaMemcpyDeviceToHost, c->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-    dev_free(tmp);
-    dev_free(ids);
-    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(fields, tmp, fb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     return IFOS_OK;
 }
 
@@ -1314,38 +1410,88 @@ extern "C" int ifos_calc_res(ifos_ctx *c, int ntr, const float *obs, const float
     if (!c || !obs || !syn || ntr < 1) return IFOS_ERR_ARG;
     CK(cudaSetDevice(c->device));
     const int ns = c->p.nt;
-    const size_t bytes = (size_t)ntr * ns * 4;
-    DevBuf d_obs, d_syn, d_diff, d_tr;
-    int rc = dev_alloc(c, d_obs, bytes);
-    if (!rc) rc = dev_alloc(c, d_syn, bytes);
-    if (!rc) rc = dev_alloc(c, d_diff, bytes);
-    if (!rc) rc = dev_alloc(c, d_tr, (size_t)2 * ntr * sizeof(double));
-    cudaError_t e = cudaSuccess;
-    if (!rc) {
-        cudaMemcpyAsync(d_obs.p, obs, bytes, cudaMemcpyHostToDevice, c->st);
-        cudaMemcpyAsync(d_syn.p, syn, bytes, cudaMemcpyHostToDevice, c->st);
-        double *tr = (double *)d_tr.p;
-        k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>((const float *)d_obs.p, (const float *)d_syn.p,
-                                                         (float *)d_diff.p, ntr, ns, c->p.dt, tr, tr + ntr);
-        c->launches++;
-        std::vector<double> h((size_t)2 * ntr);
-        if (diff) cudaMemcpyAsync(diff, d_diff.p, bytes, cudaMemcpyDeviceToHost, c->st);
-        cudaMemcpyAsync(h.data(), tr, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st);
-        e = cudaStreamSynchronize(c->st);
-        double a = 0, b = 0;
-        for (int k = 0; k < ntr; k++) {
-            a += h[k];
-            b += h[ntr + k];
-        }
-        if (l2) *l2 = a;
-        if (energy) *energy = b;
+    const size_t bytes = (size_t)ntr * ns * 4, tb = (size_t)2 * ntr * sizeof(double);
+    void *scr = nullptr;
+    if (int rc = scratch(c, tb + 3 * bytes, &scr)) return rc;
+    double *tr = (double *)scr;
+    float *d_obs = (float *)((char *)scr + tb), *d_syn = d_obs + (size_t)ntr * ns, *d_diff = d_syn + (size_t)ntr * ns;
+    CK(cudaMemcpyAsync(d_obs, obs, bytes, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(d_syn, syn, bytes, cudaMemcpyHostToDevice, c->st));
+    k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>(d_obs, d_syn, d_diff, ntr, ns, c->p.dt, tr, tr + ntr);
+    c->launches++;
+    std::vector<double> h((size_t)2 * ntr);
+    if (diff) CK(cudaMemcpyAsync(diff, d_diff, bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(h.data(), tr, tb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    double a = 0, b = 0;
+    for (int k = 0; k < ntr; k++) {
+        a += h[k];
+        b += h[ntr + k];
     }
-    dev_free(d_obs);
-    dev_free(d_syn);
-    dev_free(d_diff);
-    dev_free(d_tr);
-    if (rc) return rc;
-    if (e != cudaSuccess) return fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    if (l2) *l2 = a;
+    if (energy) *energy = b;
+    return IFOS_OK;
+}
+
+// The adjoint sources of slots [0, nshots) from their synthetic seismograms
+// (kept on the device by ifos_forward) and the observed ones: per active
+// component the residual of calc_res (src/calc_res.c, LNORM=2) is written
+// time-reversed into the staged adjoint sources, and the FP64 misfit and
+// energy are summed per slot.
+extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, double *l2, double *energy) {
+    if (!c || !obs) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    if (c->fwd_nshots < nshots) return fail(c, IFOS_ERR_STATE, "no forward seismograms for these slots");
+    CK(cudaSetDevice(c->device));
+    const ifos_params &p = c->p;
+    const int mr = std::max(1, p.max_rec), ns = p.nt;
+    // adjoint-source component -> seismogram plane (-1 unused)
+    int plane[3] = {-1, -1, -1};
+    if (c->ac || (c->psv && p.adjoint_type == 4)) {
+        plane[2] = IFOS_S_P;
+    } else {
+        if (c->psv && (p.adjoint_type == 1 || p.adjoint_type == 3)) plane[0] = IFOS_S_VX;
+        if (c->psv && (p.adjoint_type == 1 || p.adjoint_type == 2)) plane[1] = IFOS_S_VY;
+        if (c->sh) plane[2] = IFOS_S_VZ;
+    }
+    const size_t comp = (size_t)mr * ns, obs_bytes = (size_t)nshots * 3 * comp * 4;
+    const size_t tb = (size_t)nshots * 3 * mr * 2 * sizeof(double);
+    void *scr = nullptr;
+    if (int rc = scratch(c, tb + obs_bytes, &scr)) return rc;
+    double *tr = (double *)scr;
+    float *d_obs = (float *)((char *)scr + tb);
+    CK(cudaMemcpyAsync(d_obs, obs, obs_bytes, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->adj.p, 0, obs_bytes, c->st));
+    CK(cudaMemsetAsync(tr, 0, tb, c->st));
+    for (int s = 0; s < nshots; s++) {
+        const int ntr = c->ntr_h[s];
+        if (ntr < 1) continue;
+        for (int k = 0; k < 3; k++) {
+            if (plane[k] < 0) continue;
+            const float *syn = (const float *)c->sec.p + ((size_t)s * IFOS_NS + plane[k]) * comp;
+            float *adj = (float *)c->adj.p + ((size_t)s * 3 + k) * comp;
+            double *t = tr + ((size_t)s * 3 + k) * mr * 2;
+            k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>(d_obs + ((size_t)s * 3 + k) * comp, syn, adj, ntr, ns,
+                                                             p.dt, t, t + mr);
+            c->launches++;
+        }
+    }
+    std::vector<double> h(tb / sizeof(double));
+    CK(cudaMemcpyAsync(h.data(), tr, tb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int s = 0; s < nshots; s++) {
+        double a = 0, b = 0;
+        for (int k = 0; k < 3; k++) {
+            const double *t = h.data() + ((size_t)s * 3 + k) * mr * 2;
+            for (int r = 0; r < c->ntr_h[s]; r++) {
+                a += t[r];
+                b += t[mr + r];
+            }
+        }
+        if (l2) l2[s] = a;
+        if (energy) energy[s] = b;
+    }
+    c->adj_staged = true;
     return IFOS_OK;
 }
 
@@ -1468,6 +1614,36 @@ extern "C" int ifos_grad_sum_device(ifos_ctx *c, int nshots, float *dev_out) {
     c->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_set_option(ifos_ctx *c, int option, int value) {
+    if (!c) return IFOS_ERR_ARG;
+    switch (option) {
+        case IFOS_OPT_GRAPHS: c->graphs = value != 0; break;
+        case IFOS_OPT_PDL: c->pdl = value != 0; break;
+        case IFOS_OPT_BLOCKS_PER_SM:
+            if (value < 0 || value > 32) return fail(c, IFOS_ERR_ARG, "blocks per SM must be in 0..32");
+            c->blocks_per_sm = value;
+            break;
+        case IFOS_OPT_TILE_ORDER:
+            if (value != 0 && value != 1) return fail(c, IFOS_ERR_ARG, "tile order must be 0 or 1");
+            c->g.tile_order = value;
+            break;
+        default: return fail(c, IFOS_ERR_ARG, "unknown option " + std::to_string(option));
+    }
+    return IFOS_OK;
+}
+
+extern "C" int ifos_get_option(const ifos_ctx *c, int option, int *value) {
+    if (!c || !value) return IFOS_ERR_ARG;
+    switch (option) {
+        case IFOS_OPT_GRAPHS: *value = c->graphs ? 1 : 0; break;
+        case IFOS_OPT_PDL: *value = c->pdl ? 1 : 0; break;
+        case IFOS_OPT_BLOCKS_PER_SM: *value = c->blocks_per_sm; break;
+        case IFOS_OPT_TILE_ORDER: *value = c->g.tile_order; break;
+        default: return IFOS_ERR_ARG;
+    }
     return IFOS_OK;
 }
 

@@ -99,10 +99,20 @@ struct __align__(16) TileInfo {
     int pad[3];
 };
 
-__device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, TileInfo &r) {
-    const int per = ntx * nty;
-    r.slot = t / per;
-    const int rem = t - r.slot * per;
+// Tile t of a launch.  Slot-major order walks all tiles of slot 0, then of
+// slot 1, ...; slot-minor order gives consecutive t the same tile of
+// consecutive slots, so the CTAs resident at one time share the model tiles
+// of shots over the same model (one HBM read, the rest from L2).
+__device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, int nshots, int slot_minor, TileInfo &r) {
+    int rem;
+    if (slot_minor) {
+        rem = t / nshots;
+        r.slot = t - rem * nshots;
+    } else {
+        const int per = ntx * nty;
+        r.slot = t / per;
+        rem = t - r.slot * per;
+    }
     const int tyi = rem / ntx;
     r.i0 = (rem - tyi * ntx) * kTileX + 1;
     r.j0 = tyi * TY + 1;
@@ -159,7 +169,7 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
         auto issue = [&](int k, bool halo, bool plain) {
             const int st = k % NST;
             TileInfo ti;
-            tile_of(blockIdx.x + k * gridDim.x, ntx, nty, TY, ti);
+            tile_of(blockIdx.x + k * gridDim.x, ntx, nty, TY, nshots, g.tile_order, ti);
             float *stage = smem + st * P::STAGE;
             uint64_t *bar = &full[st];
             if (plain) {

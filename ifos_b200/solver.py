@@ -170,6 +170,22 @@ class ShotSolver:
                                            C.byref(en)))
         return diff, l2.value, en.value
 
+    def residual_adjoint(self, obs, nshots: int = 1):
+        """Residuals of slots [0, nshots) of the last forward run against the
+        observed seismograms ``obs`` (nshots, 3, max_rec, NT; vx, vy,
+        vz-or-p), staged as the adjoint sources of the next ``adjoint(None,
+        nshots)``.  Returns the per-slot FP64 (misfit, energy) arrays."""
+        obs = _f32(obs)
+        want = (nshots, 3, self.max_rec, self.p.nt)
+        if obs.shape != want:
+            raise ValueError(f"observed seismograms must be {want}, got {obs.shape}")
+        l2 = np.zeros(nshots, np.float64)
+        en = np.zeros(nshots, np.float64)
+        DP = C.POINTER(C.c_double)
+        self._check(self.lib.ifos_residual_adjoint(self._ctx, int(nshots), _fp(obs), l2.ctypes.data_as(DP),
+                                                   en.ctypes.data_as(DP)))
+        return l2, en
+
     def trkill_table(self, rec_xy, src_xy, lower, upper, table=None):
         """Offset-based trace-kill table (src/create_trkill_table.c): rec_xy
         (2, ntr) receiver grid indices, src_xy (2, nsrc) source coordinates in
@@ -204,6 +220,20 @@ class ShotSolver:
         """Launch on the caller's cudaStream_t (an integer handle), or on the
         context's own stream with None."""
         self._check(self.lib.ifos_set_stream(self._ctx, None if not stream_handle else C.c_void_p(stream_handle)))
+
+    def set_options(self, **opts):
+        """Execution options (``graphs``, ``pdl``, ``blocks_per_sm``,
+        ``tile_order``; see IFOS_OPT_* in include/ifos_gpu.h)."""
+        for k, v in opts.items():
+            self._check(self.lib.ifos_set_option(self._ctx, _lib.OPTIONS[k], int(v)))
+
+    def options(self) -> dict:
+        out = {}
+        for k, code in _lib.OPTIONS.items():
+            v = C.c_int()
+            self._check(self.lib.ifos_get_option(self._ctx, code, C.byref(v)))
+            out[k] = v.value
+        return out
 
     def kernel_timing(self, stride: int):
         self._check(self.lib.ifos_kernel_timing(self._ctx, int(stride)))

@@ -164,6 +164,16 @@ int ifos_dot_f64(ifos_ctx *ctx, const float *a, const float *b, size_t n, int de
 int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, float *diff, double *l2,
                   double *energy);
 
+/* The residual step between the loops (src/IFOS2D.c:2115-2180, which calls
+ * calc_res per component): for slots [0, nshots) of the last ifos_forward,
+ * forms the residual of each component the adjoint uses (vx/vy by
+ * ADJOINT_TYPE 1-3, vz for SH, p for ADJOINT_TYPE 4 / acoustic) against the
+ * observed seismograms `obs` (slot x 3 x max_rec x NT, host; components
+ * vx, vy, vz-or-p) on the device, stages them as the adjoint sources of the
+ * next ifos_adjoint(ctx, nshots, NULL, ...) and returns each slot's FP64
+ * misfit and energy in l2[nshots] / energy[nshots] (either may be NULL). */
+int ifos_residual_adjoint(ifos_ctx *ctx, int nshots, const float *obs, double *l2, double *energy);
+
 /* Offset-based trace-kill table (src/create_trkill_table.c:21-46), on the
  * device and bit-identical to the reference: killtable (ntr_glob x nsrc_glob,
  * row-major [receiver][source], host, in/out) gets 1 where the offset between
@@ -208,6 +218,28 @@ int ifos_grad_sum_device(ifos_ctx *ctx, int nshots, float *dev_out);
  * to time the library with the caller's events; NULL returns to the
  * context's own stream.  The caller keeps ownership of its stream. */
 int ifos_set_stream(ifos_ctx *ctx, void *stream);
+
+/* Execution options of a context (no counterpart in the reference; they
+ * change how the loops run, never what they compute: every setting gives
+ * bit-identical results).  A change takes effect at the next loop and
+ * discards the loops captured so far. */
+enum {
+    /* 1 (default): each time loop (ifos_forward, ifos_adjoint) is captured
+     * once into a CUDA graph per launch sequence and replayed for every
+     * later call with the same shot count; 0: launched step by step. */
+    IFOS_OPT_GRAPHS = 0,
+    /* 1 (default): the loop's kernels are programmatic dependent launches
+     * (each starts its independent loads while its predecessor drains). */
+    IFOS_OPT_PDL = 1,
+    /* persistent stencil CTAs per SM; 0 (default): as many as fit. */
+    IFOS_OPT_BLOCKS_PER_SM = 2,
+    /* 0 (default): the stencil launches walk all tiles of slot 0, then of
+     * slot 1, ...; 1: the same tile of consecutive slots on consecutive
+     * CTAs, so that shots over one model share its coefficient tiles in L2. */
+    IFOS_OPT_TILE_ORDER = 3
+};
+int ifos_set_option(ifos_ctx *ctx, int option, int value);
+int ifos_get_option(const ifos_ctx *ctx, int option, int *value);
 
 /* FP64 dot product without any device allocation.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc (code running in
