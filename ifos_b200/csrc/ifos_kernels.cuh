@@ -7,6 +7,7 @@
 // --fmad=false, so in fp32 mode each cell update rounds exactly as the
 // reference's C code does.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -508,6 +509,26 @@ __global__ void k_p_ac(KGrid g, KState<T> S, KModel<T> M) {
 // the same step changes (explosive sources, the free surface): base of the
 // snapshot of slot 0 being stored (NULL: nothing to patch), floats between
 // slots, NX*NY, and the component index of every patched field (-1 absent).
+// fp16 snapshot segments (IFOS_SNAP_F16S).  The 64 consecutive cells of a
+// row that one pipelined tile covers share a power-of-two scale 2^k, with k
+// chosen from the segment's absolute maximum so that it lands in
+// [2^14, 2^15), well inside the fp16 range (largest finite value 65504).  A
+// value v is stored as fp16(v * 2^k), rounded to nearest even, and read back
+// as float(h) * 2^-k; both scalings are exact, so fp16's rounding is the only
+// error.  k is kept as one signed byte per component, row and segment.
+constexpr int kSegCells = 64;
+__device__ __forceinline__ int seg_exponent(unsigned amax_bits) {
+    const int k = 141 - (int)(amax_bits >> 23);  // 14 - unbiased exponent of the maximum
+    return k < -126 ? -126 : (k > 126 ? 126 : k);
+}
+__device__ __forceinline__ float pow2f(int k) { return __uint_as_float((unsigned)(k + 127) << 23); }
+// all 32 lanes of a warp, each with a column pair of one segment: its k
+__device__ __forceinline__ int seg_scale_warp(float v0, float v1, bool ok0, bool ok1) {
+    const unsigned a0 = ok0 ? (__float_as_uint(v0) & 0x7fffffffu) : 0u;
+    const unsigned a1 = ok1 ? (__float_as_uint(v1) & 0x7fffffffu) : 0u;
+    return seg_exponent(__reduce_max_sync(0xffffffffu, a0 > a1 ? a0 : a1));
+}
+
 struct KSnapPatch {
     float *base;
     long long slot_floats;

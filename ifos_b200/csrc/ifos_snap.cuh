@@ -15,19 +15,91 @@ struct KSnap {
     void *base;            // slot 0, slot 0 snapshot
     long long slot_bytes;  // bytes between slots
     long long snap_bytes;  // bytes between snapshots of one slot
-    float *scale;          // [slot][snap][comp] absmax (low-precision formats)
+    float *scale;          // [slot][snap][comp] absmax (bf16 / fp16 formats)
     int ncomp, ntdtinv, format;
     int comp_plane[8];     // state plane of every component
     long long n;           // NX*NY
+    int nx, ny, segs;      // fp16 segments: row segments of kSegCells cells
+    long long ex_off;      // fp16 segments: bytes from a snapshot to its exponents [comp][NY][segs]
 };
 
 template <typename T>
 __device__ inline T snap_load(const KSnap &s, int slot, int snap, int k, long long q) {
     const char *b = (const char *)s.base + slot * s.slot_bytes + snap * s.snap_bytes;
     if (s.format == 0) return ((const T *)b)[k * s.n + q];
+    if (s.format == 3) {
+        const long long row = q / s.nx, col = q - row * s.nx;
+        const signed char e =
+            ((const signed char *)(b + s.ex_off))[((long long)k * s.ny + row) * s.segs + col / kSegCells];
+        return (T)(__half2float(((const __half *)b)[k * s.n + q]) * pow2f(-e));
+    }
     const float sc = s.scale[((long long)slot * s.ntdtinv + snap) * s.ncomp + k];
     if (s.format == 1) return (T)(__bfloat162float(((const __nv_bfloat16 *)b)[k * s.n + q]) * sc);
     return (T)(__half2float(((const __half *)b)[k * s.n + q]) * sc);
+}
+
+// fp16 segments: one warp re-quantises the row-j segment `seg` of the listed
+// components from the state planes (lane l holds cells 2l, 2l+1 of it).
+template <typename T>
+__device__ __forceinline__ void quant_seg(const KGrid &g, const KState<T> &S, const KSnap &sn, int slot, int hin,
+                                          int j, int seg, const int *comps, int ncomps) {
+    const int lane = threadIdx.x & 31;
+    const int i = seg * kSegCells + 2 * lane + 1;
+    const bool ok0 = i <= g.nx, ok1 = i + 1 <= g.nx;
+    char *b = (char *)sn.base + slot * sn.slot_bytes + hin * sn.snap_bytes;
+    __half *h = (__half *)b;
+    signed char *ex = (signed char *)(b + sn.ex_off);
+    const long long q = (long long)(j - 1) * g.nx + (i - 1);
+    for (int t = 0; t < ncomps; t++) {
+        const int k = comps[t];
+        if (k < 0) continue;
+        const T *f = fieldp(S, slot, sn.comp_plane[k]);
+        const float v0 = ok0 ? (float)f[pidx(g, j, i)] : 0.0f, v1 = ok1 ? (float)f[pidx(g, j, i + 1)] : 0.0f;
+        const int e = seg_scale_warp(v0, v1, ok0, ok1);
+        const float sc = pow2f(e);
+        if (ok0) h[k * sn.n + q] = __float2half_rn(v0 * sc);
+        if (ok1) h[k * sn.n + q + 1] = __float2half_rn(v1 * sc);
+        if (lane == 0) ex[((long long)k * g.ny + (j - 1)) * sn.segs + seg] = (signed char)e;
+    }
+}
+
+// fp16-segment snapshot store of the unpipelined paths: one warp per row
+// segment, all components.  Grid (segs, ceil(NY/8), slots), block (32, 8).
+template <typename T>
+__global__ void k_snap_seg16(KGrid g, KState<T> S, KSnap sn, int hin) {
+    pdl_wait();
+    pdl_launch();
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (j > g.ny) return;
+    const int comps[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    quant_seg<T>(g, S, sn, blockIdx.z, hin, j, blockIdx.x, comps, sn.ncomp);
+}
+
+// fp16 segments written by the stencil kernels: the free-surface and
+// explosive-source kernel changes the stresses of row 1 and of the source
+// cells after the stress kernel stored them, so those segments are stored
+// again from the final state.  Grid (segs + max_src, 1, slots), one warp.
+template <typename T>
+__global__ void k_snap_fix16(KGrid g, KState<T> S, KSnap sn, int hin, KSrc src, int surf, int4 patched) {
+    pdl_wait();
+    pdl_launch();
+    const int slot = blockIdx.z;
+    const int comps[4] = {patched.x, patched.y, patched.z, patched.w};
+    int j, seg;
+    if ((int)blockIdx.x < sn.segs) {
+        if (!surf) return;
+        j = 1;
+        seg = blockIdx.x;
+    } else {
+        const int l = blockIdx.x - sn.segs;
+        if (l >= src.nsrc[slot]) return;
+        const float *pos = src.pos + (long long)slot * 8 * src.max_src;
+        const int i = (int)pos[l];
+        j = (int)pos[src.max_src + l];
+        if (i < 1 || i > g.nx || j < 1 || j > g.ny) return;
+        seg = (i - 1) / kSegCells;
+    }
+    quant_seg<T>(g, S, sn, slot, hin, j, seg, comps, 4);
 }
 
 // fp32/fp64 snapshot copy (one thread per cell, all components)
@@ -172,7 +244,7 @@ __device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, floa
     }
 }
 
-template <int PSV, int SH, int AC>
+template <int PSV, int SH, int AC, bool F16>
 __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSnap sn, KGrad gr, int snap) {
     pdl_wait();
     pdl_launch();
@@ -185,7 +257,7 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
     if (i > g.nx) return;
     const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1), n = gr.n;
     const float *st = S.base + slot * S.slot_stride + c;
-    const float *fs = (const float *)((const char *)sn.base + slot * sn.slot_bytes + snap * sn.snap_bytes) + q;
+    const char *sb = (const char *)sn.base + slot * sn.slot_bytes + snap * sn.snap_bytes;
     float *acc = gr.acc + (long long)slot * 5 * n + q;
     auto ld2 = [](const float *p) { return *reinterpret_cast<const float2 *>(p); };
     CorrCell a0{}, a1{};
@@ -210,11 +282,25 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
         field(P_SXZ, a0.sxz, a1.sxz);
         field(P_SYZ, a0.syz, a1.syz);
     }
+    if constexpr (F16) {
+        // fp16 segments: a pair never straddles a segment (both start at odd i)
+        const __half *hs = (const __half *)sb + q;
+        const signed char *ex = (const signed char *)(sb + sn.ex_off) + (long long)(j - 1) * sn.segs + (i - 1) / kSegCells;
 #pragma unroll
-    for (int k = 0; k < NC; k++) {
-        const float2 v = ld2(fs + k * sn.n);
-        a0.f[k] = v.x;
-        a1.f[k] = v.y;
+        for (int k = 0; k < NC; k++) {
+            const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(hs + k * sn.n));
+            const float sc = pow2f(-ex[(long long)k * g.ny * sn.segs]);
+            a0.f[k] = v.x * sc;
+            a1.f[k] = v.y * sc;
+        }
+    } else {
+        const float *fs = (const float *)sb + q;
+#pragma unroll
+        for (int k = 0; k < NC; k++) {
+            const float2 v = ld2(fs + k * sn.n);
+            a0.f[k] = v.x;
+            a1.f[k] = v.y;
+        }
     }
     const long long mo = (long long)M.slot_model[slot] * M.model_stride + c;
     float2 mm{0, 0}, ll{0, 0}, rho{0, 0}, u{0, 0};

@@ -109,7 +109,7 @@ struct ifos_ctx {
     // snapshots
     bool with_snap = false;
     int ncomp = 0, comp_plane[8] = {0};
-    long long snap_bytes = 0, snap_slot_bytes = 0;
+    long long snap_bytes = 0, snap_slot_bytes = 0, snap_ex_off = 0;
     bool snaps_valid = false;
     int fwd_nshots = 0;
     // host mirrors
@@ -247,7 +247,7 @@ static int check_params(const ifos_params &p, std::string &why) {
     if (p.seismo < 0 || p.seismo > 5) return bad("SEISMO must be 0..5");
     if (p.max_shots < 1 || p.max_models < 1) return bad("max_shots and max_models must be >= 1");
     if (p.max_src < 0 || p.max_rec < 0) return bad("max_src/max_rec must be >= 0");
-    if (p.snap_format < 0 || p.snap_format > 2) return bad("snap_format must be 0, 1 or 2");
+    if (p.snap_format < 0 || p.snap_format > 3) return bad("snap_format must be 0, 1, 2 or 3");
     if (p.precision < 0 || p.precision > 1) return bad("precision must be 0 or 1");
     if (!(p.dt > 0) || !(p.dh > 0)) return bad("DT and DH must be positive");
     for (int l = 0; l < p.L; l++)
@@ -259,7 +259,8 @@ struct Layout {
     long long pitch, rows, plane, slot_elems, psix, psiy, psi_slot, model_elems;
     int nfield, nmem, nmodel;
     long long snap_bytes_per, snap_slot_bytes;
-    int ncomp;
+    long long snap_ex_off;  // fp16 segments: bytes from a snapshot to its exponents
+    int ncomp, segs;
 };
 
 static Layout layout_of(const ifos_params &p) {
@@ -283,6 +284,12 @@ static Layout layout_of(const ifos_params &p) {
     L.ncomp = (psv ? (p.acoustic ? 3 : 5) : 0) + (sh ? 3 : 0);
     const int bytes = p.snap_format == 0 ? (p.precision ? 8 : 4) : 2;
     L.snap_bytes_per = (long long)L.ncomp * p.nx * p.ny * bytes;
+    L.segs = (p.nx + 63) / 64;
+    if (p.snap_format == IFOS_SNAP_F16S) {
+        // halves [comp][NY*NX], then one exponent byte per component, row and segment
+        L.snap_ex_off = (L.snap_bytes_per + 15) / 16 * 16;
+        L.snap_bytes_per = (L.snap_ex_off + (long long)L.ncomp * p.ny * L.segs + 255) / 256 * 256;
+    }
     L.snap_slot_bytes = L.snap_bytes_per * (p.nt / p.dtinv);
     return L;
 }
@@ -405,7 +412,7 @@ static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     t.snap_ncomp = c->ncomp;
     for (int k = 0; k < NP_FIELD; k++) t.snap_comp[k] = -1;
     for (int k = 0; k < c->ncomp; k++) t.snap_comp[c->comp_plane[k]] = k;
-    c->fused_snap = c->with_snap && c->p.snap_format == 0;
+    c->fused_snap = c->with_snap && (c->p.snap_format == IFOS_SNAP_F32 || c->p.snap_format == IFOS_SNAP_F16S);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
         c->num_sms = sms;
@@ -533,6 +540,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     }
     c->snap_bytes = L.snap_bytes_per;
     c->snap_slot_bytes = L.snap_slot_bytes;
+    c->snap_ex_off = L.snap_ex_off;
 
     const size_t e = c->esz;
     const int S = p.max_shots;
@@ -560,6 +568,10 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     if ((rc = dev_alloc(c, c->dot_out, 2 * sizeof(double)))) return bail(rc);
     if (c->with_snap) {
         if ((rc = dev_alloc(c, c->snap, (size_t)S * L.snap_slot_bytes))) return bail(rc);
+        // components a loop never writes (vxp1/vyp1 of the FDORDER 10/12
+        // branches) read as zero, as the reference's zeroed arrays do
+        if (cudaMemsetAsync(c->snap.p, 0, (size_t)S * L.snap_slot_bytes, c->st) != cudaSuccess)
+            return bail(fail(c, IFOS_ERR_CUDA, "snapshot clear failed"));
         if ((rc = dev_alloc(c, c->snap_scale, (size_t)S * (p.nt / p.dtinv) * c->ncomp * sizeof(float) + 4)))
             return bail(rc);
     }
@@ -810,6 +822,10 @@ static KSnap ksnap(const ifos_ctx *c) {
     s.format = c->p.snap_format;
     for (int k = 0; k < 8; k++) s.comp_plane[k] = c->comp_plane[k];
     s.n = (long long)c->p.nx * c->p.ny;
+    s.nx = c->p.nx;
+    s.ny = c->p.ny;
+    s.segs = (c->p.nx + 63) / 64;
+    s.ex_off = c->snap_ex_off;
     return s;
 }
 
@@ -865,10 +881,13 @@ struct Launcher {
     KSnapOut snap_out(int hin) const {
         KSnapOut so{};
         if (hin >= 0) {
-            so.base = (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes);
-            so.slot_floats = c->snap_slot_bytes / 4;
+            so.base = (char *)c->snap.p + (size_t)hin * c->snap_bytes;
+            so.slot_bytes = c->snap_slot_bytes;
             so.n = (long long)c->p.nx * c->p.ny;
             so.pairs = (c->p.nx % 2) == 0;
+            so.f16 = c->p.snap_format == IFOS_SNAP_F16S;
+            so.ex_off = c->snap_ex_off;
+            so.segs = (c->p.nx + 63) / 64;
         }
         return so;
     }
@@ -1120,14 +1139,17 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     CK(cudaMemsetAsync(c->bad.p, 0, 4, c->st));
     const bool snaps = store && c->with_snap;
     const int ntd = p.nt / p.dtinv;
-    if (snaps && p.snap_format != 0)
+    if (snaps && (p.snap_format == IFOS_SNAP_BF16 || p.snap_format == IFOS_SNAP_F16))
         CK(cudaMemsetAsync(c->snap_scale.p, 0, (size_t)nshots * ntd * c->ncomp * 4, c->st));
     const bool force = (c->psv && !c->ac && any_force_source(c, nshots)) || c->sh ||
                        (c->ac && any_force_source(c, nshots));
     KSnap sn = ksnap(c);
-    // fp32 snapshots stored by the stencil kernels; the source and surface
-    // kernels patch the cells they change afterwards
+    // snapshots stored by the stencil kernels; the source and surface kernel
+    // patches the fp32 cells it changes afterwards, and the fp16 segments
+    // holding them are stored again after it
     const bool fused = snaps && c->pipe && c->fused_snap;
+    const bool f16s = p.snap_format == IFOS_SNAP_F16S;
+    const int segs = (p.nx + 63) / 64;
     KSnapPatch pt{};
     pt.slot_floats = c->snap_slot_bytes / 4;
     pt.n = (long long)p.nx * p.ny;
@@ -1147,7 +1169,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
         const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
         const int fhin = (fused && snap_now) ? hin : -1;
-        pt.base = fhin >= 0 ? (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes) : nullptr;
+        pt.base = (fhin >= 0 && !f16s) ? (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes) : nullptr;
         {
             KTimer t(c, 0, sample);
             Lr.v_step(0, snap_now ? 1 : 0, fhin);
@@ -1163,10 +1185,20 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         }
         Lr.post_fwd(nt, c->psv != 0, pt);
         if (snap_now && fused) {
+            if (f16s && (p.free_surf || c->psv)) {
+                const int4 patched = make_int4(pt.c_sxx, pt.c_syy, pt.c_sp, pt.c_syz);
+                launch_dep(c->st, c->pdl, k_snap_fix16<T>, dim3(segs + std::max(1, p.max_src), 1, nshots), dim3(32),
+                           0, c->g, Lr.S, sn, hin, Lr.src, p.free_surf ? 1 : 0, patched);
+                c->launches++;
+            }
             hin++;
         } else if (snap_now) {
             KTimer t(c, 2, sample);
-            if (p.snap_format == 0) {
+            if (f16s) {
+                launch_dep(c->st, c->pdl, k_snap_seg16<T>, dim3(segs, (p.ny + 7) / 8, nshots), dim3(32, 8), 0, c->g,
+                           Lr.S, sn, hin);
+                c->launches++;
+            } else if (p.snap_format == 0) {
                 launch_dep(c->st, c->pdl, k_snap_store<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.S, sn, hin);
                 c->launches++;
             } else {
@@ -1229,13 +1261,24 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
             KTimer t(c, 3, sample);
             bool pairs = false;
             if constexpr (std::is_same<T, float>::value) {
-                if (p.snap_format == 0 && p.nx % 2 == 0) {
+                const bool f16s = p.snap_format == IFOS_SNAP_F16S;
+                if ((p.snap_format == IFOS_SNAP_F32 || f16s) && p.nx % 2 == 0) {
                     const dim3 gc((unsigned)((p.nx / 2 + 127) / 128), (unsigned)p.ny, (unsigned)nshots);
                     const int h = ntd - hin_a;
-                    if (c->ac) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 0, 1>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
-                    else if (c->psv && c->sh) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 1, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
-                    else if (c->psv) launch_dep(c->st, c->pdl, k_correlate_pairs<1, 0, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
-                    else launch_dep(c->st, c->pdl, k_correlate_pairs<0, 1, 0>, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    auto corr = [&](auto kern) {
+                        launch_dep(c->st, c->pdl, kern, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
+                    };
+                    if (f16s) {
+                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, true>);
+                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, true>);
+                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, true>);
+                        else corr(k_correlate_pairs<0, 1, 0, true>);
+                    } else {
+                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, false>);
+                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, false>);
+                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, false>);
+                        else corr(k_correlate_pairs<0, 1, 0, false>);
+                    }
                     pairs = true;
                 }
             }

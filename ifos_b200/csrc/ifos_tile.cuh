@@ -66,10 +66,15 @@ struct KMaps {
 // fp32 snapshot written by a launch: snapshot of slot 0 being stored (NULL:
 // none), floats between slots, NX*NY, and whether rows start 8-byte aligned
 // (NX even) for pair stores.
+// the snapshot a stencil launch stores (base NULL: none)
 struct KSnapOut {
-    float *base;
-    long long slot_floats, n;
-    int pairs;
+    char *base;            // this snapshot of slot 0
+    long long slot_bytes;  // bytes between slots
+    long long n;           // NX*NY
+    int pairs;             // NX even: column pairs are aligned for vector stores
+    int f16;               // fp16 segments (IFOS_SNAP_F16S); else fp32
+    long long ex_off;      // fp16: bytes from a snapshot to its exponents [comp][NY][segs]
+    int segs;              // fp16: segments per row
 };
 
 // NH halo boxes, NP loaded plain boxes, NO output-only plain boxes, NST stages
@@ -366,26 +371,56 @@ __device__ __forceinline__ void gput2(float *p, float n0, float n1, bool pair, b
 // Row addresses of a thread's column pair: the cell (j, i) in the state of a
 // slot and, on snapshot steps, in the snapshot being stored.
 struct RowOut {
-    float *st;  // state plane 0 at (j, i)
-    float *sn;  // snapshot component 0 at (j, i), NULL when not storing
+    float *st;          // state plane 0 at (j, i)
+    float *sn;          // fp32 snapshot component 0 at (j, i), NULL when not storing fp32
+    __half *sh;         // fp16 snapshot component 0 at (j, i), NULL when not storing fp16
+    signed char *se;    // fp16: exponent of component 0 for this row segment
+    long long se_comp;  // fp16: exponents between components
     bool pair, v0, spair;
     __device__ __forceinline__ RowOut(const KGrid &g, const KState<float> &S, const KSnapOut &so, int slot, int j,
                                       const Cols &cl) {
         st = S.base + (long long)slot * S.slot_stride + ((j - 1 + HY) * g.pitch + (cl.i - 1 + HX));
-        sn = so.base ? so.base + slot * so.slot_floats + ((long long)(j - 1) * g.nx + (cl.i - 1)) : nullptr;
+        sn = nullptr;
+        sh = nullptr;
+        se = nullptr;
+        se_comp = 0;
+        if (so.base) {
+            char *b = so.base + slot * so.slot_bytes;
+            const long long q = (long long)(j - 1) * g.nx + (cl.i - 1);
+            if (so.f16) {
+                sh = reinterpret_cast<__half *>(b) + q;
+                se = reinterpret_cast<signed char *>(b + so.ex_off) + (long long)(j - 1) * so.segs +
+                     (cl.i - 1) / kSegCells;
+                se_comp = (long long)g.ny * so.segs;
+            } else {
+                sn = reinterpret_cast<float *>(b) + q;
+            }
+        }
         pair = cl.v1;
         v0 = cl.v0;
         spair = cl.v1 && so.pairs;
     }
     __device__ __forceinline__ void put(long long off, float n0, float n1) const { gput2(st + off, n0, n1, pair, v0); }
+    // every lane of the warp calls this for its column pair of the row
     __device__ __forceinline__ void snap(long long n, int comp, float n0, float n1) const {
-        if (sn && comp >= 0) {
+        if (comp < 0) return;
+        if (sn) {
             float *p = sn + comp * n;
             if (spair) *reinterpret_cast<float2 *>(p) = make_float2(n0, n1);
             else {
                 if (v0) p[0] = n0;
                 if (pair) p[1] = n1;
             }
+        } else if (sh) {
+            const int k = seg_scale_warp(n0, n1, v0, pair);
+            const float s = pow2f(k);
+            __half *p = sh + comp * n;
+            if (spair) *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(n0 * s, n1 * s);
+            else {
+                if (v0) p[0] = __float2half_rn(n0 * s);
+                if (pair) p[1] = __float2half_rn(n1 * s);
+            }
+            if (threadIdx.x == 0) se[comp * se_comp] = (signed char)k;
         }
     }
 };
@@ -788,7 +823,7 @@ struct OpVPsv {
             const RowOut out(g, S, so, slot, j, cl);
             out.put(S.off[P_VX], o[0][0], o[0][1]);
             out.put(S.off[P_VY], o[1][0], o[1][1]);
-            if (!QUIRK && (SW == 1 || (P1 && !out.sn))) {
+            if (!QUIRK && (SW == 1 || (P1 && !out.sn && !out.sh))) {
                 out.put(S.off[P_VXP1], o[2][0], o[2][1]);
                 out.put(S.off[P_VYP1], o[3][0], o[3][1]);
             }

@@ -71,6 +71,10 @@ enum {
 #define IFOS_SNAP_F32 0
 #define IFOS_SNAP_BF16 1 /* bf16 with one fp32 scale per snapshot and component */
 #define IFOS_SNAP_F16 2  /* fp16 with one fp32 scale per snapshot and component */
+/* fp16 with a power-of-two scale per snapshot, component and 64-cell row
+ * segment, written by the stencil kernels themselves (no extra pass over the
+ * wavefield); the scale puts each segment's maximum in [2^14, 2^15). */
+#define IFOS_SNAP_F16S 3
 
 /* Parameters: the reference's global scalars of the propagation path
  * (src/globvar.h; read by src/update_v_PML.c:41-48, src/PML_pro.c:88-98,

@@ -1,0 +1,66 @@
+"""Autotuner: candidate sets, the cache, and (on the GPU) that the tuned
+options are among the timed ones and keep results bit-identical."""
+import json
+
+import numpy as np
+import pytest
+
+from ifos_b200 import autotune as A
+from ifos_b200.params import ShotParams
+
+
+def test_candidates_cover_the_knobs():
+    one = A.candidates(1)
+    many = A.candidates(4)
+    assert {c["tile_order"] for c in one} == {0}
+    assert {c["tile_order"] for c in many} == {0, 1}
+    assert {c["blocks_per_sm"] for c in many} == {0, 1, 2}
+    assert {c["pdl"] for c in many} == {0, 1}
+    assert len(many) == 2 * len(one)
+
+
+def test_short_run_keeps_the_snapshot_interval():
+    p = ShotParams(nx=64, ny=40, nt=900, dtinv=3)
+    q = A.short_params(p)
+    assert q.nt % q.dtinv == 0 and q.nt < p.nt and (q.nx, q.ny, q.dtinv) == (64, 40, 3)
+
+
+def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
+    monkeypatch.setenv("IFOS_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(A, "_device_name", lambda d: "fake")
+    calls = []
+
+    def fake_time(p, model, nshots, options, snap_format="fp32", device=0, reps=3):
+        options = list(options)
+        calls.append(len(options))
+        return [(10.0 + o["blocks_per_sm"] + 0.5 * o["tile_order"] - 0.25 * o["pdl"], o) for o in options]
+
+    monkeypatch.setattr(A, "time_options", fake_time)
+    p = ShotParams(nx=64, ny=40, nt=90, dtinv=3)
+    best = A.tune(p, {}, nshots=4)
+    assert best == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=0)
+    again = A.tune(p, {}, nshots=4)
+    assert again == best and calls == [12]  # second call served from the cache
+    data = json.load(open(tmp_path / "tune.json"))
+    assert len(data) == 1 and len(next(iter(data.values()))["timed"]) == 12
+
+
+@pytest.mark.gpu
+def test_tuned_options_run_and_match(tmp_path, monkeypatch):
+    monkeypatch.setenv("IFOS_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from ifos_b200.solver import ShotSolver
+    from tests.golden.cases import build_case
+    from tests.gpu_helpers import bit_equal
+    p, model, g, sig, adj = build_case("psv_el_o4")
+    best = A.tune(p, model, nshots=2)
+    timed = json.load(open(tmp_path / "tune.json"))
+    assert best in [{k: v for k, v in t.items() if k != "ms"} for t in next(iter(timed.values()))["timed"]]
+    res = []
+    for opts in ({}, best):
+        with ShotSolver(p, max_rec=g.recpos.shape[1]) as s:
+            s.set_options(**opts)
+            s.upload_model(model)
+            s.setup_shot(0, g.srcpos, sig, g.recpos)
+            sec = s.forward(1)
+            res.append((sec, s.adjoint(adj[None])))
+    assert bit_equal(res[0][0], res[1][0]) and bit_equal(res[0][1], res[1][1])
