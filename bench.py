@@ -1,17 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the shot solver on its headline workload.
 
-Workload (one "step" = one shot-gradient: the forward time loop with
-snapshot storage plus the adjoint time loop with the zero-lag correlation and
-the per-shot gradient assembly) on the viscoelastic layered case: 2000 x 600
-grid, DH 2 m, FDORDER 8 Holberg (0.1 %), L=3 relaxation mechanisms fit to
-Q=20 over 5-60 Hz, 12 seeded layers + 3 dipping faults, 400 receivers, Ricker
-15 Hz, NT 6000, DTINV 3, FP32 arithmetic, FP32 snapshots (48 GB per shot).
+Workload (one "step" = one batch of B shot-gradients: the forward time loop
+with snapshot storage plus the adjoint time loop with the zero-lag
+correlation and the per-shot gradient assembly) on the viscoelastic layered
+case: 2000 x 600 grid, DH 2 m, FDORDER 8 Holberg (0.1 %), L=3 relaxation
+mechanisms fit to Q=20 over 5-60 Hz, 12 seeded layers + 3 dipping faults,
+400 receivers, Ricker 15 Hz, NT 6000, DTINV 3, FP32 arithmetic.  ``value``
+is the batched low-precision-snapshot form (B shots per context, fp16
+snapshots with per-segment scales, CUDA-graph time loops; B and the
+execution options from the autotuner); ``plain_fp32`` is the drop-in path
+(one shot, fp32 snapshots, step-by-step launches) on the same workload.
 Shots cycle over the 64 seeded source positions.  All data are synthetic
-(seeded numpy); the state (~0.2 GB) and the snapshots (48 GB) are far larger
-than L2, so no flush is needed between steps.
+(seeded numpy); the state (~0.2 GB) and the snapshots (tens of GB per shot)
+are far larger than L2, so no flush is needed between steps.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--snap bf16]
+Also reported: the batched form on its own workload (256 shots over 5
+models, 400 x 160), the serving form (a Poisson stream of mixed requests at
+50-150 % of saturation), the precision form (errors against an fp64 run on
+the 4000 x 1200 grid), and the reference's CPU code on the host cores.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--snap fp16s]
 
 Prints one JSON line on rank 0.  ``value`` is device-timed (CUDA events on
 the stream the library launches on) with inputs resident in HBM; ``e2e``
@@ -47,11 +56,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--snap", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--snap", default="fp16s", choices=["fp32", "bf16", "fp16", "fp16s"],
+                    help="snapshot format of the batched form (the plain FP32 path always stores fp32)")
+    ap.add_argument("--batch", type=int, default=0, help="shots per context (0: chosen by the autotuner)")
+    ap.add_argument("--max-batch", type=int, default=8)
     ap.add_argument("--nt", type=int, default=6000, help="time steps (6000 is the workload; smaller only for tests)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-full", action="store_true", help="full-size serving stream (grids to 3000x1000)")
     return ap.parse_args()
 
 
@@ -212,9 +228,14 @@ def cpu_baseline(full_nt, procs=None, ns=30):
 
 
 # ---------------------------------------------------------------------------
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def fp64_error(p, model, g, nt=300):
-    """Error of the fp32 (and low-precision snapshot) path against the same
-    kernels in fp64 on a truncated run of the workload grid (untimed)."""
+    """Error of the fp32 path and of each snapshot format against the same
+    kernels in fp64 arithmetic with fp64 snapshots, on a truncated run of the
+    workload grid (untimed)."""
     from ifos_b200 import workloads as W
     from ifos_b200.solver import ShotSolver
     q = p.copy(nt=nt)
@@ -224,25 +245,229 @@ def fp64_error(p, model, g, nt=300):
     adj = (rng.standard_normal((1, 3, ntr, nt)) * 1e-6).astype(np.float32)
     out = {}
     for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
-                    ("fp16", dict(snap_format="fp16"))):
+                    ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s"))):
         with ShotSolver(q, max_rec=ntr, **kw) as s:
             s.upload_model(model)
             s.setup_shot(0, g.srcpos, sig, g.recpos)
             sec = s.forward(1, store=True)[0]
             gr = s.adjoint(adj)[0]
         out[tag] = (sec.astype(np.float64), gr.astype(np.float64))
-
-    def rel(a, b):
-        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-
     ref_s, ref_g = out["fp64"]
-    res = {"run": f"same grid, NT={nt}, fp64 arithmetic as the oracle"}
-    for tag in ("fp32", "bf16", "fp16"):
+    res = {"run": f"workload grid, NT={nt}, against fp64 arithmetic with fp64 snapshots"}
+    for tag in ("fp32", "bf16", "fp16", "fp16s"):
         s_, g_ = out[tag]
-        res[tag] = {"seismogram_rel_l2": rel(s_[:2], ref_s[:2]), "gradient_rel_l2": rel(g_[3:6], ref_g[3:6]),
+        res[tag] = {"seismogram_rel_l2": _rel(s_[:2], ref_s[:2]), "gradient_rel_l2": _rel(g_[3:6], ref_g[3:6]),
                     "misfit_rel": abs(float(np.sum(s_[:2] ** 2)) - float(np.sum(ref_s[:2] ** 2))) /
                     float(np.sum(ref_s[:2] ** 2))}
     return res
+
+
+def precision_study(device, nt=1200):
+    """The precision form on its own grid (4000 x 1200, DH 2.5 m, FDORDER 8,
+    layered + faulted + 15 % random-field model): P-SV and SH gradients with
+    fp32, bf16, fp16 and fp16-segment snapshots against an fp64 run (fp64
+    arithmetic and snapshots) of the same kernels.  The misfit is the FP64
+    device misfit of the residual against seeded observed data; the gradient
+    is driven by that residual.  NT is truncated so that the fp64 run's
+    snapshots fit one GPU."""
+    from ifos_b200 import workloads as W
+    from ifos_b200.solver import ShotSolver
+    out = {"run": f"4000x1200 precision grid, NT={nt}, DTINV 20, one mid-line shot per wave type"}
+    for wave, name, planes, comps in ((1, "psv", [3, 4, 5], [0, 1]), (2, "sh", [8, 9], [2])):
+        p, model, geoms = W.precision_layered(0, nt=nt, wavetype=wave)
+        g = geoms[len(geoms) // 2]
+        sig = W.ricker(p, g.srcpos)
+        ntr = g.recpos.shape[1]
+        rng = np.random.default_rng(7 + wave)
+        obs = (rng.standard_normal((1, 3, ntr, p.nt)) * 1e-9).astype(np.float32)
+        runs = {}
+        for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
+                        ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s"))):
+            with ShotSolver(p, max_rec=ntr, device=device, **kw) as s:
+                s.upload_model(model)
+                s.setup_shot(0, g.srcpos, sig, g.recpos)
+                sec = s.forward(1, store=True)[0]
+                l2, _ = s.residual_adjoint(obs, 1)
+                gr = s.adjoint(None, 1)[0]
+            runs[tag] = (sec[comps].astype(np.float64), gr[planes].astype(np.float64), float(l2[0]))
+        rs, rg, rm = runs["fp64"]
+        out[name] = {tag: {"seismogram_rel_l2": _rel(runs[tag][0], rs), "gradient_rel_l2": _rel(runs[tag][1], rg),
+                           "misfit_rel": abs(runs[tag][2] - rm) / max(abs(rm), 1e-300)}
+                     for tag in ("fp32", "bf16", "fp16", "fp16s")}
+    return out
+
+
+def _timed_shots(solver, stream, nshots, run):
+    """Device milliseconds of `run()` on the solver's stream (CUDA events)."""
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    run()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1)
+
+
+def plain_path(p, models, shots, device, count=2, warmup=1):
+    """The drop-in path as the reference driver would use it: one shot per
+    context, fp32 snapshots, every kernel launched step by step (no graph
+    replay, default options).  Returns shot-gradients/s."""
+    import torch
+    from ifos_b200 import workloads as W
+    from ifos_b200.solver import ShotSolver
+    ntr = max(g.recpos.shape[1] for _, g in shots)
+    stream = torch.cuda.current_stream(device)
+    rng = np.random.default_rng(3)
+    adj = (rng.standard_normal((1, 3, ntr, p.nt)) * 1e-6).astype(np.float32)
+    with ShotSolver(p, max_rec=ntr, max_models=len(models), device=device) as s:
+        s.set_options(graphs=0)
+        for i, m in enumerate(models):
+            s.upload_model(m, i)
+        s.set_stream(stream.cuda_stream)
+        s.stage_adjoint(adj)
+
+        def shot(k):
+            mi, g = shots[k % len(shots)]
+            s.setup_shot(0, g.srcpos, W.ricker(p, g.srcpos), g.recpos, model=mi)
+            s.forward(1, store=True, fetch=False)
+            s.adjoint(None, 1, fetch=False)
+
+        for k in range(warmup):
+            shot(k)
+
+        def run():
+            for k in range(count):
+                shot(warmup + k)
+
+        ms = _timed_shots(s, stream, count, run)
+        s.set_stream(None)
+    return {"value": count / (ms / 1e3), "unit": METRIC, "shots": count, "ms_per_shot": ms / count,
+            "form": "1 shot per context, fp32 snapshots, step-by-step launches"}
+
+
+def batched_form(device, snap, max_batch=128):
+    """The batched form on its workload: 256 shots round-robin over the
+    plain-elastic start model (400 x 160, FDORDER 4, NT 2000) and 4 seeded
+    perturbations of it, stepped B at a time in one context (B and the
+    execution options from the autotuner, memory permitting), low-precision
+    snapshots, CUDA-graph time loops; against the plain FP32 path on the same
+    shots."""
+    import torch
+    from ifos_b200 import autotune as A
+    from ifos_b200 import workloads as W
+    from ifos_b200.solver import ShotSolver
+    p, true, models, shots = W.batched_perturbed(0, nshots=256)
+    ntr = max(g.recpos.shape[1] for _, g in shots)
+    plain = plain_path(p, models, shots, device, count=4)
+    free = torch.cuda.mem_get_info(device)[0]
+    choice = A.best_batch(p, models[0], int(free * 0.8), max_batch=max_batch, snap_format=snap, device=device,
+                          sizes=[16, 32, 64, 128])
+    B = choice["nshots"]
+    stream = torch.cuda.current_stream(device)
+    rng = np.random.default_rng(5)
+    adj = (rng.standard_normal((B, 3, ntr, p.nt)) * 1e-6).astype(np.float32)
+    sigs = [W.ricker(p, g.srcpos) for _, g in shots]
+    with ShotSolver(p, max_shots=B, max_models=len(models), max_rec=ntr, snap_format=snap, device=device) as s:
+        s.set_options(**choice["options"])
+        for i, m in enumerate(models):
+            s.upload_model(m, i)
+        s.set_stream(stream.cuda_stream)
+        s.stage_adjoint(adj, B)
+
+        def batch(b0):
+            n = min(B, len(shots) - b0)
+            for k in range(n):
+                mi, g = shots[b0 + k]
+                s.setup_shot(k, g.srcpos, sigs[b0 + k], g.recpos, model=mi)
+            s.forward(n, store=True, fetch=False)
+            s.adjoint(None, n, fetch=False)
+
+        batch(0)  # captures the graphs
+
+        def run():
+            for b0 in range(0, len(shots), B):
+                batch(b0)
+
+        ms = _timed_shots(s, stream, len(shots), run)
+        s.set_stream(None)
+    value = len(shots) / (ms / 1e3)
+    return {"workload": "batched plain-elastic 400x160 FDORDER4 NT2000 DTINV2, 256 shots over 5 models",
+            "value": value, "unit": METRIC, "batch": B, "snapshots": snap, "options": choice["options"],
+            "ms_all_shots": ms, "plain_fp32": plain, "speedup_vs_plain_fp32": value / plain["value"]}
+
+
+def serving_bench(device, snap, full=False, n_requests=32, loads=(0.5, 1.0, 1.5)):
+    """The serving form: a Poisson stream of mixed shot requests (70 %
+    gradients, 30 % forward-only) over six seeded surveys with different
+    grids, NT, FDORDER (4/8) and physics (elastic / viscoelastic L=3), served
+    by one persistent ShotServer (continuous batching, HBM admission).  The
+    saturation throughput is measured with all requests queued at once; the
+    stream is then replayed at 50 %, 100 % and 150 % of it, and p50/p99
+    latency (arrival to result on the host) and throughput are reported."""
+    import threading
+
+    from ifos_b200 import workloads as W
+    from ifos_b200.serving import ShotRequest, ShotServer
+    if full:
+        surveys = W.serving_surveys(0, 6, (300, 3000), (1000, 8000))
+    else:
+        surveys = W.serving_surveys(0, 6, (300, 1200), (600, 2400))
+    sig_cache = {}
+
+    def make(entry, k):
+        _, si, x, kind = entry
+        sv = surveys[si]
+        p = sv.params
+        src = W.source_rows(p, x, 3 * p.dh, fc=15.0)
+        key = (si, x)
+        if key not in sig_cache:
+            sig_cache[key] = W.ricker(p, src)
+        rng = np.random.default_rng(1000 + k)
+        obs = (rng.standard_normal((3, sv.rec.shape[1], p.nt)) * 1e-9).astype(np.float32) if kind == "gradient" \
+            else None
+        return ShotRequest(params=p, model=sv.model, model_id=sv.model_id, srcpos=src, signals=sig_cache[key],
+                           recpos=sv.rec, kind=kind, observed=obs, snap_format=snap)
+
+    out = {"workload": ("full-size" if full else "scaled") + " serving stream: 6 surveys, grids " +
+           ", ".join(f"{s.params.nx}x{s.params.ny}/NT{s.params.nt}/O{s.params.fdorder}/L{s.params.L}"
+                     for s in surveys), "requests_per_run": n_requests, "snapshots": snap}
+    with ShotServer(device=device, max_batch=8, lanes=3, paused=True) as srv:
+        # warm-up: every survey's contexts, models and graphs become resident
+        warm = [make((0.0, si, float(surveys[si].xs[0]), kind), 10_000 + 2 * si + (kind == "gradient"))
+                for si in range(len(surveys)) for kind in ("forward", "gradient")]
+        futs = [srv.submit(r) for r in warm]
+        srv.resume()
+        for f in futs:
+            f.result()
+        # saturation: the whole stream queued at once
+        stream = W.serving_stream(surveys, n_requests, 0.0, seed=1)
+        reqs = [make(e, k) for k, e in enumerate(stream)]
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        futs = [srv.submit(r) for r in reqs]
+        for f in futs:
+            f.result()
+        sat_s = time.perf_counter() - t0
+        sat = n_requests / sat_s
+        out["saturation"] = {"throughput_req_s": sat, **srv.stats()}
+        for load in loads:
+            rate = load * sat
+            stream = W.serving_stream(surveys, n_requests, rate, seed=int(load * 100))
+            reqs = [make(e, k) for k, e in enumerate(stream)]
+            srv.reset_stats()
+            futs = []
+            t0 = time.perf_counter()
+            for (t_arr, *_), r in zip(stream, reqs):
+                delay = t0 + t_arr - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                futs.append(srv.submit(r))
+            for f in futs:
+                f.result()
+            st = srv.stats()
+            out[f"load_{int(load * 100)}pct"] = {"offered_req_s": rate, **st}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -283,18 +508,13 @@ def main():
     device = local
     torch.cuda.set_device(device)
 
+    from ifos_b200 import autotune as A
     from ifos_b200 import workloads as W
     from ifos_b200.solver import ShotSolver
 
     p, model, geoms = workload(args.nt)
     ntr = max(g.recpos.shape[1] for g in geoms)
-    solver = ShotSolver(p, max_rec=ntr, snap_format=args.snap, device=device)
-    solver.upload_model(model)
-    stream = torch.cuda.current_stream(device)
-    solver.set_stream(stream.cuda_stream)
-    rng = np.random.default_rng(100 + rank)
-    adj_host = (rng.standard_normal((1, 3, ntr, p.nt)) * 1e-6).astype(np.float32)
-    solver.stage_adjoint(adj_host)
+    cells = p.nx * p.ny
     sigs = {}
 
     def shot(k):
@@ -304,14 +524,36 @@ def main():
             sigs[idx] = W.ricker(p, g.srcpos)
         return g, sigs[idx]
 
+    # ---- the plain FP32 path (drop-in form), for the speed-up of the batched form ----
+    plain = None
+    if not args.no_plain:
+        plain = plain_path(p, [model], [(0, geoms[(rank + world * k) % len(geoms)]) for k in range(3)], device)
+
+    # ---- the batched, low-precision-snapshot form: batch size and options tuned ----
+    if args.batch > 0:
+        B, opts = args.batch, A.tune(p, model, args.batch, args.snap, device)
+    else:
+        free = torch.cuda.mem_get_info(device)[0]
+        choice = A.best_batch(p, model, int(free * 0.85), max_batch=args.max_batch, snap_format=args.snap,
+                              device=device)
+        B, opts = choice["nshots"], choice["options"]
+    solver = ShotSolver(p, max_shots=B, max_rec=ntr, snap_format=args.snap, device=device)
+    solver.set_options(**opts)
+    solver.upload_model(model)
+    stream = torch.cuda.current_stream(device)
+    solver.set_stream(stream.cuda_stream)
+    rng = np.random.default_rng(100 + rank)
+    adj_host = (rng.standard_normal((B, 3, ntr, p.nt)) * 1e-6).astype(np.float32)
+    solver.stage_adjoint(adj_host, B)
     grad_dev = torch.zeros((5, p.ny, p.nx), dtype=torch.float32, device=f"cuda:{device}")
 
     def one_step(k):
-        g, sig = shot(k)
-        solver.setup_shot(0, g.srcpos, sig, g.recpos)
-        solver.forward(1, store=True, fetch=False)
+        for b in range(B):
+            g, sig = shot(k * B + b)
+            solver.setup_shot(b, g.srcpos, sig, g.recpos)
+        solver.forward(B, store=True, fetch=False)
         t_f = solver.last_ms
-        solver.adjoint(None, 1, fetch=False)
+        solver.adjoint(None, B, fetch=False)
         return t_f + solver.last_ms
 
     for k in range(args.warmup):
@@ -329,7 +571,7 @@ def main():
         for k in range(args.steps):
             step_ms.append(one_step(args.warmup + k))
         if dist:
-            solver.grad_sum_device(1, grad_dev.data_ptr())
+            solver.grad_sum_device(B, grad_dev.data_ptr())
             dist.all_reduce(grad_dev)
         ev1.record(stream)
         torch.cuda.synchronize(device)
@@ -344,24 +586,26 @@ def main():
         t = torch.tensor([elapsed], device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-    total_shots = args.steps * world
+    total_shots = args.steps * B * world
     value = total_shots / (elapsed / 1000.0)
-    cells = p.nx * p.ny
 
-    # ---- end-to-end through the host-buffer API ----
+    # ---- end to end through the public API with host buffers ----
     e2e = None
     if not args.no_e2e:
-        sec_bytes = 6 * ntr * p.nt * 4
-        grad_bytes = 10 * cells * 4
+        obs_host = (np.random.default_rng(200 + rank).standard_normal((B, 3, ntr, p.nt)) * 1e-9).astype(np.float32)
         e2e_times = []
-        g = sig = None
+        h2d = 0
         for k in range(args.steps):
-            g, sig = shot(args.warmup + args.steps + k)
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
-            solver.setup_shot(0, g.srcpos, sig, g.recpos)
-            solver.forward(1, store=True, fetch=True)
-            solver.adjoint(adj_host, 1, fetch=True)
+            h2d = obs_host.nbytes
+            for b in range(B):
+                g, sig = shot((args.warmup + args.steps + k) * B + b)
+                solver.setup_shot(b, g.srcpos, sig, g.recpos)
+                h2d += g.srcpos.nbytes + sig.nbytes + g.recpos.nbytes
+            sec = solver.forward(B, store=True, fetch=True)
+            l2, _ = solver.residual_adjoint(obs_host, B)
+            grads = solver.adjoint(None, B, fetch=True)
             torch.cuda.synchronize(device)
             e2e_times.append(time.perf_counter() - t0)
         tot = sum(e2e_times)
@@ -369,12 +613,12 @@ def main():
             t = torch.tensor([tot], device=f"cuda:{device}", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             tot = float(t.item())
-        h2d = int(g.srcpos.nbytes + sig.nbytes + g.recpos.nbytes + adj_host.nbytes)
-        e2e = {"value": total_shots / tot, "unit": METRIC, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(sec_bytes + grad_bytes)}
+        e2e = {"value": total_shots / tot, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(sec.nbytes + grads.nbytes + l2.nbytes),
+               "path": "ShotSolver.setup_shot / forward(fetch) / residual_adjoint(observed) / adjoint(fetch)"}
+    solver.close()
 
     if rank != 0:
-        solver.close()
         if dist:
             dist.destroy_process_group()
         return 0
@@ -384,17 +628,19 @@ def main():
     s_ms, s_n = ktimes["stress"]
     v_ms, v_n = ktimes["velocity"]
     avg_s = s_ms / max(1, s_n)
-    b_s = stress_bytes(p)
+    b_s = stress_bytes(p) * B  # one launch steps all B slots
     achieved = b_s / (avg_s / 1000.0) / 1e9 if s_n else None
     tr = ncu_traffic()
-    traffic = tr[0] * cells / tr[1] if tr else None
-    roof = {"kernel": "viscoelastic stress update (L=3 memory variables + CPML), fp32", "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+    traffic = tr[0] * cells * B / tr[1] if tr else None
+    roof = {"kernel": f"viscoelastic stress update (L=3 memory variables + CPML), fp32, {B} shot(s) per launch",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
             "fallback 6650 GB/s",
-            "traffic": traffic, "alg_bytes_per_launch": b_s, "avg_launch_ms": avg_s, "sampled_launches": s_n,
+            "traffic": traffic, "traffic_source": "ncu capture of one single-shot launch, scaled by cells x shots",
+            "alg_bytes_per_launch": b_s, "avg_launch_ms": avg_s, "sampled_launches": s_n,
             "velocity_kernel": {"avg_launch_ms": v_ms / max(1, v_n),
-                                "achieved_gbs": (velocity_bytes(p, False) + velocity_bytes(p, True)) / 2 /
+                                "achieved_gbs": B * (velocity_bytes(p, False) + velocity_bytes(p, True)) / 2 /
                                 (v_ms / max(1, v_n) / 1000.0) / 1e9 if v_n else None}}
     extra = {}
     if not args.no_error:
@@ -402,6 +648,17 @@ def main():
             extra["fp64_error"] = fp64_error(p, model, geoms[0])
         except Exception as exc:  # report, never hide
             extra["fp64_error"] = {"error": repr(exc)}
+    if world == 1:
+        for name, flag, fn in (("batched_form", args.no_batched, lambda: batched_form(device, args.snap)),
+                               ("serving", args.no_serving,
+                                lambda: serving_bench(device, args.snap, full=args.serving_full)),
+                               ("precision", args.no_error, lambda: precision_study(device))):
+            if flag:
+                continue
+            try:
+                extra[name] = fn()
+            except Exception as exc:
+                extra[name] = {"error": repr(exc)}
     cpu = None
     if not args.no_cpu and world == 1:
         cpu = cpu_baseline(p.nt)
@@ -411,13 +668,15 @@ def main():
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy models, sources, residuals)",
         "config": {"workload": WORKLOAD, "grid": [p.nx, p.ny], "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
-                   "dtinv": p.dtinv, "snapshots": args.snap, "shots_per_step_per_gpu": 1,
-                   "parallelism": f"shots sharded over {world} GPU(s)",
-                   "l2": "inputs larger than L2 (48 GB snapshots + 0.2 GB state per shot); no flush"},
+                   "dtinv": p.dtinv, "snapshots": args.snap, "shots_per_step_per_gpu": B,
+                   "execution_options": opts, "parallelism": f"shots sharded over {world} GPU(s)",
+                   "l2": "inputs larger than L2 (snapshots of tens of GB + 0.2 GB state per shot); no flush"},
         "gcell_updates_per_s": 2 * cells * p.nt * total_shots / (elapsed / 1000.0) / 1e9,
         "latency_ms": {"p50": lat[len(lat) // 2],
                        "p99": lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)],
-                       "per": "shot-gradient (forward + adjoint)"},
+                       "per": f"step of {B} shot-gradient(s) (forward + adjoint)"},
+        "plain_fp32": plain,
+        "speedup_vs_plain_fp32": value / plain["value"] if plain else None,
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
@@ -426,7 +685,6 @@ def main():
         **extra,
     }
     print(json.dumps(line), flush=True)
-    solver.close()
     if dist:
         dist.destroy_process_group()
     return 0

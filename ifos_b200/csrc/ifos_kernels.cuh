@@ -510,23 +510,30 @@ __global__ void k_p_ac(KGrid g, KState<T> S, KModel<T> M) {
 // snapshot of slot 0 being stored (NULL: nothing to patch), floats between
 // slots, NX*NY, and the component index of every patched field (-1 absent).
 // fp16 snapshot segments (IFOS_SNAP_F16S).  The 64 consecutive cells of a
-// row that one pipelined tile covers share a power-of-two scale 2^k, with k
-// chosen from the segment's absolute maximum so that it lands in
-// [2^14, 2^15), well inside the fp16 range (largest finite value 65504).  A
-// value v is stored as fp16(v * 2^k), rounded to nearest even, and read back
-// as float(h) * 2^-k; both scalings are exact, so fp16's rounding is the only
-// error.  k is kept as one signed byte per component, row and segment.
+// row that one pipelined tile covers share one fp32 scale: the segment's
+// absolute maximum m is mapped to kSegTop, just below fp16's largest finite
+// value (65504), so the segment's largest values sit at the top of fp16's
+// top binade, where its relative precision is best.  A value v is stored as
+// fp16(v * (kSegTop / m)), rounded to nearest even, and read back as
+// float(h) * (m / kSegTop); a segment whose maximum is below 1e-30 (or NaN)
+// is stored as zeros.
 constexpr int kSegCells = 64;
-__device__ __forceinline__ int seg_exponent(unsigned amax_bits) {
-    const int k = 141 - (int)(amax_bits >> 23);  // 14 - unbiased exponent of the maximum
-    return k < -126 ? -126 : (k > 126 ? 126 : k);
-}
-__device__ __forceinline__ float pow2f(int k) { return __uint_as_float((unsigned)(k + 127) << 23); }
-// all 32 lanes of a warp, each with a column pair of one segment: its k
-__device__ __forceinline__ int seg_scale_warp(float v0, float v1, bool ok0, bool ok1) {
+constexpr float kSegTop = 65472.0f;  // 2^15 (2 - 2^-9)
+// all 32 lanes of a warp, each with a column pair of one segment: its maximum |v|
+__device__ __forceinline__ float seg_absmax_warp(float v0, float v1, bool ok0, bool ok1) {
     const unsigned a0 = ok0 ? (__float_as_uint(v0) & 0x7fffffffu) : 0u;
     const unsigned a1 = ok1 ? (__float_as_uint(v1) & 0x7fffffffu) : 0u;
-    return seg_exponent(__reduce_max_sync(0xffffffffu, a0 > a1 ? a0 : a1));
+    return __uint_as_float(__reduce_max_sync(0xffffffffu, a0 > a1 ? a0 : a1));
+}
+// the quantisation factor q and the stored read-back scale of a segment maximum m
+__device__ __forceinline__ void seg_scales(float m, float &q, float &inv) {
+    if (m >= 1e-30f) {
+        q = kSegTop / m;
+        inv = m / kSegTop;
+    } else {
+        q = 0.0f;
+        inv = 0.0f;
+    }
 }
 
 struct KSnapPatch {

@@ -20,7 +20,7 @@ struct KSnap {
     int comp_plane[8];     // state plane of every component
     long long n;           // NX*NY
     int nx, ny, segs;      // fp16 segments: row segments of kSegCells cells
-    long long ex_off;      // fp16 segments: bytes from a snapshot to its exponents [comp][NY][segs]
+    long long ex_off;      // fp16 segments: bytes from a snapshot to its scales [comp][NY][segs]
 };
 
 template <typename T>
@@ -29,9 +29,8 @@ __device__ inline T snap_load(const KSnap &s, int slot, int snap, int k, long lo
     if (s.format == 0) return ((const T *)b)[k * s.n + q];
     if (s.format == 3) {
         const long long row = q / s.nx, col = q - row * s.nx;
-        const signed char e =
-            ((const signed char *)(b + s.ex_off))[((long long)k * s.ny + row) * s.segs + col / kSegCells];
-        return (T)(__half2float(((const __half *)b)[k * s.n + q]) * pow2f(-e));
+        const float sc = ((const float *)(b + s.ex_off))[((long long)k * s.ny + row) * s.segs + col / kSegCells];
+        return (T)(__half2float(((const __half *)b)[k * s.n + q]) * sc);
     }
     const float sc = s.scale[((long long)slot * s.ntdtinv + snap) * s.ncomp + k];
     if (s.format == 1) return (T)(__bfloat162float(((const __nv_bfloat16 *)b)[k * s.n + q]) * sc);
@@ -48,18 +47,18 @@ __device__ __forceinline__ void quant_seg(const KGrid &g, const KState<T> &S, co
     const bool ok0 = i <= g.nx, ok1 = i + 1 <= g.nx;
     char *b = (char *)sn.base + slot * sn.slot_bytes + hin * sn.snap_bytes;
     __half *h = (__half *)b;
-    signed char *ex = (signed char *)(b + sn.ex_off);
+    float *ex = (float *)(b + sn.ex_off);
     const long long q = (long long)(j - 1) * g.nx + (i - 1);
     for (int t = 0; t < ncomps; t++) {
         const int k = comps[t];
         if (k < 0) continue;
         const T *f = fieldp(S, slot, sn.comp_plane[k]);
         const float v0 = ok0 ? (float)f[pidx(g, j, i)] : 0.0f, v1 = ok1 ? (float)f[pidx(g, j, i + 1)] : 0.0f;
-        const int e = seg_scale_warp(v0, v1, ok0, ok1);
-        const float sc = pow2f(e);
-        if (ok0) h[k * sn.n + q] = __float2half_rn(v0 * sc);
-        if (ok1) h[k * sn.n + q + 1] = __float2half_rn(v1 * sc);
-        if (lane == 0) ex[((long long)k * g.ny + (j - 1)) * sn.segs + seg] = (signed char)e;
+        float qf, inv;
+        seg_scales(seg_absmax_warp(v0, v1, ok0, ok1), qf, inv);
+        if (ok0) h[k * sn.n + q] = __float2half_rn(v0 * qf);
+        if (ok1) h[k * sn.n + q + 1] = __float2half_rn(v1 * qf);
+        if (lane == 0) ex[((long long)k * g.ny + (j - 1)) * sn.segs + seg] = inv;
     }
 }
 
@@ -285,11 +284,11 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
     if constexpr (F16) {
         // fp16 segments: a pair never straddles a segment (both start at odd i)
         const __half *hs = (const __half *)sb + q;
-        const signed char *ex = (const signed char *)(sb + sn.ex_off) + (long long)(j - 1) * sn.segs + (i - 1) / kSegCells;
+        const float *ex = (const float *)(sb + sn.ex_off) + (long long)(j - 1) * sn.segs + (i - 1) / kSegCells;
 #pragma unroll
         for (int k = 0; k < NC; k++) {
             const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(hs + k * sn.n));
-            const float sc = pow2f(-ex[(long long)k * g.ny * sn.segs]);
+            const float sc = ex[(long long)k * g.ny * sn.segs];
             a0.f[k] = v.x * sc;
             a1.f[k] = v.y * sc;
         }

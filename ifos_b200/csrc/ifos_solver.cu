@@ -137,6 +137,7 @@ struct ifos_ctx {
     bool graphs = true;     // time loops captured once and replayed as CUDA graphs
     int blocks_per_sm = 0;  // persistent stencil CTAs per SM (0: as many as fit)
     cudaStream_t cap_st = nullptr;  // capture stream (the caller's may be the legacy default stream)
+    bool capturing = false;         // a loop is being captured: timing events become graph nodes
     LoopGraph gfwd, gadj;
 };
 
@@ -157,13 +158,13 @@ struct KTimer {
     KTimer(ifos_ctx *cc, int k, bool sample) : c(cc), cls(k) {
         if (!(sample && cc->prof_stride > 0)) return;
         e0 = pool_event(c);
-        if (e0) cudaEventRecord(e0, c->st);
+        if (e0) cudaEventRecordWithFlags(e0, c->st, c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
     }
     ~KTimer() {
         if (!e0) return;
         cudaEvent_t e1 = pool_event(c);
         if (!e1) return;
-        cudaEventRecord(e1, c->st);
+        cudaEventRecordWithFlags(e1, c->st, c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
         c->ev_pairs.push_back({cls, e0, e1});
     }
 };
@@ -173,6 +174,8 @@ static void collect_kernel_times(ifos_ctx *c) {
         if (cudaEventElapsedTime(&ms, pr.e0, pr.e1) == cudaSuccess) {
             c->kt_ms[pr.cls] += ms;
             c->kt_n[pr.cls]++;
+        } else {
+            cudaGetLastError();  // an unusable sample is dropped, not reported later
         }
     }
     c->ev_pairs.clear();
@@ -286,9 +289,9 @@ static Layout layout_of(const ifos_params &p) {
     L.snap_bytes_per = (long long)L.ncomp * p.nx * p.ny * bytes;
     L.segs = (p.nx + 63) / 64;
     if (p.snap_format == IFOS_SNAP_F16S) {
-        // halves [comp][NY*NX], then one exponent byte per component, row and segment
+        // halves [comp][NY*NX], then one fp32 scale per component, row and segment
         L.snap_ex_off = (L.snap_bytes_per + 15) / 16 * 16;
-        L.snap_bytes_per = (L.snap_ex_off + (long long)L.ncomp * p.ny * L.segs + 255) / 256 * 256;
+        L.snap_bytes_per = (L.snap_ex_off + (long long)L.ncomp * p.ny * L.segs * 4 + 255) / 256 * 256;
     }
     L.snap_slot_bytes = L.snap_bytes_per * (p.nt / p.dtinv);
     return L;
@@ -1092,7 +1095,9 @@ static int run_loop(ifos_ctx *c, LoopGraph &lg, const std::string &key, F &&enqu
         c->st = c->cap_st;
         cudaError_t e = cudaStreamBeginCapture(c->cap_st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
+            c->capturing = true;
             enqueue();
+            c->capturing = false;
             cudaGraph_t g = nullptr;
             e = cudaStreamEndCapture(c->cap_st, &g);
             if (e == cudaSuccess) {
@@ -1407,6 +1412,32 @@ extern "C" int ifos_fetch_fields(ifos_ctx *c, int slot, float *fields) {
     if (slot < 0 || slot >= c->p.max_shots) return fail(c, IFOS_ERR_ARG, "slot out of range");
     CK(cudaSetDevice(c->device));
     return c->dbl ? fetch_fields_t<double>(c, slot, fields) : fetch_fields_t<float>(c, slot, fields);
+}
+
+template <typename T>
+__global__ void k_snap_out(KSnap sn, int slot, int snap, float *out) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= sn.n) return;
+    for (int k = 0; k < sn.ncomp; k++) out[k * sn.n + q] = (float)snap_load<T>(sn, slot, snap, k, q);
+}
+
+extern "C" int ifos_fetch_snapshot(ifos_ctx *c, int slot, int index, float *out) {
+    if (!c || !out) return IFOS_ERR_ARG;
+    if (!c->with_snap) return fail(c, IFOS_ERR_STATE, "context has no snapshots");
+    if (slot < 0 || slot >= c->p.max_shots || index < 0 || index >= c->p.nt / c->p.dtinv)
+        return fail(c, IFOS_ERR_ARG, "slot or snapshot index out of range");
+    CK(cudaSetDevice(c->device));
+    const long long N = (long long)c->p.nx * c->p.ny;
+    const size_t bytes = (size_t)c->ncomp * N * 4;
+    void *tmp = nullptr;
+    if (int rc = scratch(c, bytes, &tmp)) return rc;
+    const unsigned nb = (unsigned)((N + 255) / 256);
+    if (c->dbl) k_snap_out<double><<<nb, 256, 0, c->st>>>(ksnap(c), slot, index, (float *)tmp);
+    else k_snap_out<float><<<nb, 256, 0, c->st>>>(ksnap(c), slot, index, (float *)tmp);
+    c->launches++;
+    CK(cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
 }
 
 extern "C" int ifos_forward_steps(ifos_ctx *c, int nsteps, float *fields) {

@@ -73,7 +73,7 @@ struct KSnapOut {
     long long n;           // NX*NY
     int pairs;             // NX even: column pairs are aligned for vector stores
     int f16;               // fp16 segments (IFOS_SNAP_F16S); else fp32
-    long long ex_off;      // fp16: bytes from a snapshot to its exponents [comp][NY][segs]
+    long long ex_off;      // fp16: bytes from a snapshot to its segment scales [comp][NY][segs]
     int segs;              // fp16: segments per row
 };
 
@@ -374,8 +374,8 @@ struct RowOut {
     float *st;          // state plane 0 at (j, i)
     float *sn;          // fp32 snapshot component 0 at (j, i), NULL when not storing fp32
     __half *sh;         // fp16 snapshot component 0 at (j, i), NULL when not storing fp16
-    signed char *se;    // fp16: exponent of component 0 for this row segment
-    long long se_comp;  // fp16: exponents between components
+    float *se;          // fp16: scale of component 0 for this row segment
+    long long se_comp;  // fp16: scales between components
     bool pair, v0, spair;
     __device__ __forceinline__ RowOut(const KGrid &g, const KState<float> &S, const KSnapOut &so, int slot, int j,
                                       const Cols &cl) {
@@ -389,8 +389,7 @@ struct RowOut {
             const long long q = (long long)(j - 1) * g.nx + (cl.i - 1);
             if (so.f16) {
                 sh = reinterpret_cast<__half *>(b) + q;
-                se = reinterpret_cast<signed char *>(b + so.ex_off) + (long long)(j - 1) * so.segs +
-                     (cl.i - 1) / kSegCells;
+                se = reinterpret_cast<float *>(b + so.ex_off) + (long long)(j - 1) * so.segs + (cl.i - 1) / kSegCells;
                 se_comp = (long long)g.ny * so.segs;
             } else {
                 sn = reinterpret_cast<float *>(b) + q;
@@ -412,15 +411,15 @@ struct RowOut {
                 if (pair) p[1] = n1;
             }
         } else if (sh) {
-            const int k = seg_scale_warp(n0, n1, v0, pair);
-            const float s = pow2f(k);
+            float q, inv;
+            seg_scales(seg_absmax_warp(n0, n1, v0, pair), q, inv);
             __half *p = sh + comp * n;
-            if (spair) *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(n0 * s, n1 * s);
+            if (spair) *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(n0 * q, n1 * q);
             else {
-                if (v0) p[0] = __float2half_rn(n0 * s);
-                if (pair) p[1] = __float2half_rn(n1 * s);
+                if (v0) p[0] = __float2half_rn(n0 * q);
+                if (pair) p[1] = __float2half_rn(n1 * q);
             }
-            if (threadIdx.x == 0) se[comp * se_comp] = (signed char)k;
+            if (threadIdx.x == 0) se[comp * se_comp] = inv;
         }
     }
 };

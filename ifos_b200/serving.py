@@ -223,6 +223,12 @@ class ShotServer:
     def __exit__(self, *exc):
         self.close()
 
+    def reset_stats(self):
+        """Forget the results recorded so far (the pool stays resident)."""
+        with self._cv:
+            self._results = []
+            self.max_inflight = self._running
+
     def stats(self) -> dict:
         with self._cv:
             res = list(self._results)

@@ -146,6 +146,14 @@ class ShotSolver:
         self._check(self.lib.ifos_forward_steps(self._ctx, int(nsteps), _fp(out)))
         return out
 
+    def snapshot(self, index: int, slot: int = 0):
+        """Stored forward snapshot ``index`` as the correlation reads it
+        (ncomp, NY, NX), dequantised for the 2-byte formats."""
+        ncomp = (0 if self.p.wavetype == 2 else (3 if self.p.acoustic else 5)) + (3 if self.p.wavetype != 1 else 0)
+        out = np.zeros((ncomp, self.p.ny, self.p.nx), np.float32)
+        self._check(self.lib.ifos_fetch_snapshot(self._ctx, int(slot), int(index), _fp(out)))
+        return out
+
     def fields(self, slot=0):
         out = np.zeros((NF, self.p.ny, self.p.nx), np.float32)
         self._check(self.lib.ifos_fetch_fields(self._ctx, int(slot), _fp(out)))

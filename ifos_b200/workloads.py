@@ -277,3 +277,60 @@ def read_model(prefix: str, nx: int, ny: int) -> dict:
         a = np.fromfile(f"{prefix}.{key}", dtype=np.float32, count=nx * ny)
         out[key] = np.ascontiguousarray(a.reshape(nx, ny).T)
     return out
+
+
+@dataclass
+class Survey:
+    """One acquisition a serving stream draws shot requests from."""
+    params: ShotParams
+    model: dict
+    model_id: str
+    xs: np.ndarray  # source x positions (m)
+    rec: np.ndarray
+
+
+def serving_surveys(seed: int = 0, count: int = 6, nx_range=(300, 3000), nt_range=(1000, 8000)):
+    """Surveys of the serving form: grids uniform between nx_range[0] x
+    nx_range[0]/3 and nx_range[1] x nx_range[1]/3 (300 x 100 to 3000 x 1000 at
+    full size), NT uniform in nt_range (multiples of 100), FDORDER 4 or 8,
+    elastic or viscoelastic L=3, each on a seeded layered model, 100
+    receivers at 3 cells depth, DTINV 3."""
+    rng = np.random.default_rng(seed)
+    out = []
+    fl, tau = qfit_tau(3, 20.0, 5.0, 60.0)
+    for k in range(count):
+        nx = int(rng.integers(nx_range[0] // 10, nx_range[1] // 10 + 1)) * 10
+        ny = max(60, nx // 3)
+        nt = int(rng.integers(nt_range[0] // 300, nt_range[1] // 300 + 1)) * 300
+        fd = int(rng.choice([4, 8]))
+        visco = bool(rng.uniform() < 0.5)
+        p = ShotParams(nx=nx, ny=ny, nt=nt, dh=2.0, fdorder=fd, maxrelerror=1 if fd == 8 else 0, fw=20,
+                       free_surf=1, boundary=0, vppml=1500.0, fpml=15.0, npower=2.0, k_max_pml=1.0,
+                       L=3 if visco else 0, fl=fl if visco else [], tau=tau if visco else 0.0,
+                       f_ref=15.0 if visco else 0.0, wavetype=1, seismo=1, source_type=1, adjoint_type=1, dtinv=3,
+                       source_shape=1)
+        vp = layered_faulted(rng, nx, ny, 8, 1500.0, 4000.0, 2, p.dh)
+        model = {"vp": vp, "vs": (vp / np.float32(1.73)).astype(np.float32), "rho": gardner_rho(vp)}
+        vmax = float(vp.max()) * (math.sqrt(1.0 + 3 * tau) if visco else 1.0)
+        coeffs = _HOLBERG_01[8] if fd == 8 else _TAYLOR[4]
+        p.dt = cfl_dt(p.dh, vmax, sum(abs(c) for c in coeffs))
+        margin = p.fw + 5
+        xr = np.linspace(margin, nx - margin, 100)
+        rec = receiver_rows(p, xr * p.dh, np.full(xr.shape, 3 * p.dh))
+        out.append(Survey(p, model, f"survey{seed}-{k}", np.linspace(margin, nx - margin, 64) * p.dh, rec))
+    return out
+
+
+def serving_stream(surveys, n_requests: int, rate_hz: float, seed: int = 0, gradient_frac: float = 0.7):
+    """A Poisson stream of shot requests over `surveys`: (arrival time in s,
+    survey index, source x in m, kind), 70 % forward + adjoint gradients and
+    30 % forward-only modelling by default."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n_requests)) if rate_hz > 0 else np.zeros(n_requests)
+    out = []
+    for k in range(n_requests):
+        s = int(rng.integers(0, len(surveys)))
+        x = float(rng.choice(surveys[s].xs))
+        kind = "gradient" if rng.uniform() < gradient_frac else "forward"
+        out.append((float(t[k]), s, x, kind))
+    return out

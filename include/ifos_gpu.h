@@ -71,9 +71,9 @@ enum {
 #define IFOS_SNAP_F32 0
 #define IFOS_SNAP_BF16 1 /* bf16 with one fp32 scale per snapshot and component */
 #define IFOS_SNAP_F16 2  /* fp16 with one fp32 scale per snapshot and component */
-/* fp16 with a power-of-two scale per snapshot, component and 64-cell row
- * segment, written by the stencil kernels themselves (no extra pass over the
- * wavefield); the scale puts each segment's maximum in [2^14, 2^15). */
+/* fp16 with an fp32 scale per snapshot, component and 64-cell row segment,
+ * written by the stencil kernels themselves (no extra pass over the
+ * wavefield); the scale maps each segment's maximum to 65472. */
 #define IFOS_SNAP_F16S 3
 
 /* Parameters: the reference's global scalars of the propagation path
@@ -155,6 +155,11 @@ int ifos_grad_sum(ifos_ctx *ctx, int nshots, float *out);
 /* Run `nsteps` forward steps of slot 0 from zero state without snapshots and
  * copy the IFOS_NF field planes to `fields` (parity checks of single steps). */
 int ifos_forward_steps(ifos_ctx *ctx, int nsteps, float *fields);
+/* Stored forward snapshot `index` (0 .. NT/DTINV-1) of `slot`, read back as
+ * the correlation reads it (dequantised for the 2-byte formats): ncomp x NY x
+ * NX floats, components in the order vxp1, vyp1, sxx, syy, sxy (P-SV; acoustic
+ * vxp1, vyp1, p), then vzp1, sxz, syz (SH). */
+int ifos_fetch_snapshot(ifos_ctx *ctx, int slot, int index, float *out);
 /* Copy the current IFOS_NF field planes of `slot` to host. */
 int ifos_fetch_fields(ifos_ctx *ctx, int slot, float *fields);
 

@@ -217,3 +217,36 @@ def test_device_residual_equals_calc_res_per_component(case):
     assert bit_equal(g_dev, g_host)
     assert l2[0] == pytest.approx(tot_l2, rel=1e-12) and en[0] == pytest.approx(tot_en, rel=1e-12)
     assert l2[0] > 0
+
+
+def _seg_max(a):
+    """max |a| over each 64-cell row segment, broadcast back to the cells."""
+    *lead, nx = a.shape
+    segs = (nx + 63) // 64
+    pad = np.zeros((*lead, segs * 64))
+    pad[..., :nx] = np.abs(a)
+    m = pad.reshape(*lead, segs, 64).max(axis=-1)
+    return np.repeat(m, 64, axis=-1)[..., :nx]
+
+
+@pytest.mark.parametrize("case", ["psv_el_o4", "psv_visc_o8_holberg", "sh_visc_o4", "acoustic_o4_p"])
+def test_fp16_segment_snapshots_round_within_half_an_ulp(case):
+    """Every stored fp16-segment value is the fp32 snapshot value scaled so
+    that its segment's maximum m maps to 65472 and rounded to fp16:
+    |stored - v| <= 2^-11 |v| (plus the two fp32 scalings) in fp16's normal
+    range and half a subnormal ulp, 2^-25 * m / 65472, below it; segments
+    whose maximum is below 1e-30 are stored as zeros."""
+    p, model, g, sig, adj = build_case(case)
+    snaps = {}
+    for fmt in ("fp32", "fp16s"):
+        with ShotSolver(p, max_rec=g.recpos.shape[1], snap_format=fmt) as s:
+            s.upload_model(model)
+            s.setup_shot(0, g.srcpos, sig, g.recpos)
+            s.forward(1, store=True, fetch=False)
+            snaps[fmt] = np.stack([s.snapshot(k) for k in range(p.nt // p.dtinv)]).astype(np.float64)
+    a, b = snaps["fp32"], snaps["fp16s"]
+    m = _seg_max(a)
+    bound = 2.0 ** -11 * (1 + 2.0 ** -10) * np.abs(a) + m * 2.0 ** -40 + np.where(m < 1e-30, m, 0.0)
+    bad = np.abs(b - a) > bound
+    assert not bad.any(), (int(bad.sum()), np.argwhere(bad)[:5].tolist())
+    assert np.abs(a).max() > 0
