@@ -1647,6 +1647,44 @@ extern "C" int ifos_time_window(ifos_ctx *c, int ntr, int ns, float *sections, i
     return IFOS_OK;
 }
 
+// The parabola fit of the line search (src/calc_opt_step.c:73-112): the
+// misfits of the three test steps define a + b e + c e^2, solved by Gaussian
+// elimination without pivoting in the order of src/solvelin.c:55-68; the
+// step is the extremum -b/(2c) with the reference's clamps.
+template <typename T>
+static float opt_step_t(const float *l2t, const float *epst) {
+    T A[3][3], b[3], x[3];
+    for (int i = 0; i < 3; i++) {
+        A[i][2] = (T)epst[i] * (T)epst[i];
+        A[i][1] = (T)epst[i];
+        A[i][0] = (T)1.0;
+        b[i] = (T)l2t[i];
+    }
+    for (int k = 0; k < 2; k++)
+        for (int n = k; n < 2; n++) {
+            const T a = A[n + 1][k] / A[k][k];
+            for (int m = 0; m < 3; m++) A[n + 1][m] = A[n + 1][m] - a * A[k][m];
+            b[n + 1] = b[n + 1] - a * b[k];
+        }
+    for (int k = 2; k >= 0; k--) {
+        T c = b[k];
+        for (int m = 2; m >= k + 1; m--) c = c - A[k][m] * x[m];
+        x[k] = c / A[k][k];
+    }
+    // the reference divides in double (2.0 is a double literal)
+    float opteps = (float)(-(double)x[1] / (2.0 * (double)x[2]));
+    if ((2.0 * (double)x[2]) < 0.0 && l2t[1] > l2t[2]) opteps = epst[2];
+    if (opteps > epst[2]) opteps = epst[2];
+    if (opteps < 0.0f) opteps = epst[0];
+    return opteps;
+}
+
+extern "C" int ifos_opt_step(const float *l2t, const float *epst, int fp64, float *opteps) {
+    if (!l2t || !epst || !opteps) return IFOS_ERR_ARG;
+    *opteps = fp64 ? opt_step_t<double>(l2t, epst) : opt_step_t<float>(l2t, epst);
+    return IFOS_OK;
+}
+
 extern "C" int ifos_fd_coeffs(const ifos_params *p, float *hc7) {
     if (!p || !hc7) return IFOS_ERR_ARG;
     return fd_coefficients(p->fdorder, p->maxrelerror, hc7) ? IFOS_OK : IFOS_ERR_ARG;

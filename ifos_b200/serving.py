@@ -96,8 +96,9 @@ def shape_key(req: ShotRequest):
 class GpuBackend:
     """Backend on the CUDA library: one ShotSolver per context."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, tune: bool = True):
         self.device = device
+        self.tune = tune
 
     def total_bytes(self) -> int:
         import torch
@@ -111,10 +112,19 @@ class GpuBackend:
                                        max_src=max_src, max_rec=max_rec, snap_format=snap_format)
 
     def create(self, p: ShotParams, kind: str, nshots: int, max_models: int, max_src: int, max_rec: int,
-               snap_format: str):
+               snap_format: str, model: Optional[dict] = None):
+        """A context for the batch; its execution options come from the
+        autotuner (timed once per shape and batch size, then cached)."""
         from .solver import ShotSolver
-        return ShotSolver(p, max_shots=nshots, max_models=max_models, max_src=max_src, max_rec=max_rec,
-                          snapshots=(kind == GRADIENT), snap_format=snap_format, device=self.device)
+        opts = {}
+        if self.tune and model is not None and kind == GRADIENT:
+            from . import autotune
+            opts = autotune.tune(p, model, nshots, snap_format, self.device)
+        s = ShotSolver(p, max_shots=nshots, max_models=max_models, max_src=max_src, max_rec=max_rec,
+                       snapshots=(kind == GRADIENT), snap_format=snap_format, device=self.device)
+        if opts:
+            s.set_options(**opts)
+        return s
 
     @staticmethod
     def run(ctx, reqs: List[ShotRequest], model_index: List[int]) -> List[dict]:
@@ -177,6 +187,7 @@ class ShotServer:
         self._ids = itertools.count()
         self._closed = False
         self._paused = bool(paused)
+        self._closing: list = []
         self._results: List[ShotResult] = []
         self.peak_bytes = 0
         self.max_inflight = 0
@@ -213,9 +224,11 @@ class ShotServer:
             for t in list(self._threads):
                 t.join()
         with self._cv:
-            for c in self._pool:
-                self.backend.close(c.handle)
+            handles = [c.handle for c in self._pool if c.handle is not None] + self._closing
             self._pool.clear()
+            self._closing = []
+        for h in handles:
+            self.backend.close(h)
 
     def __enter__(self):
         return self
@@ -257,6 +270,14 @@ class ShotServer:
     def _loop(self):
         with self._cv:
             while True:
+                if self._closing:
+                    handles, self._closing = self._closing, []
+                    self._cv.release()
+                    try:
+                        for h in handles:
+                            self.backend.close(h)
+                    finally:
+                        self._cv.acquire()
                 while not self._ready():
                     self._cv.wait()
                 if not self._pending:  # closed and drained
@@ -271,11 +292,11 @@ class ShotServer:
                         continue
                     self._cv.wait()  # until a running batch frees memory
                     continue
-                ctx, batch = plan
+                ctx, batch, victims = plan
                 ctx.busy = True
                 self._running += 1
                 self.max_inflight = max(self.max_inflight, self._running)
-                t = threading.Thread(target=self._run_batch, args=(ctx, batch), daemon=True)
+                t = threading.Thread(target=self._run_batch, args=(ctx, batch, victims), daemon=True)
                 self._threads.append(t)
                 t.start()
         for t in list(self._threads):
@@ -292,20 +313,22 @@ class ShotServer:
         idle = [c for c in self._pool if c.key == key and not c.busy and c.max_src >= nsrc and c.max_rec >= ntr]
         best = max(idle, key=lambda c: c.nshots) if idle else None
         if best is not None and best.nshots >= len(same):
-            return best, self._take(same, best)
+            return best, self._take(same, best), []
         # a new, larger context: as many of the waiting shots as fit
         n, floor = len(same), (best.nshots if best is not None else 0)
         while n > floor:
             need = self.backend.bytes_needed(head.params, head.kind, n, self.max_models, nsrc, ntr, head.snap_format)
             if self._make_room(need, keep=best):
-                handle = self.backend.create(head.params, head.kind, n, self.max_models, nsrc, ntr, head.snap_format)
-                c = _Context(key, handle, n, self.max_models, nsrc, ntr, need)
+                # created by the batch's own thread, after it has released the evicted contexts
+                c = _Context(key, None, n, self.max_models, nsrc, ntr, need)
+                c.spec = (head.params, head.kind, n, self.max_models, nsrc, ntr, head.snap_format, head.model)
                 self._pool.append(c)
                 self.peak_bytes = max(self.peak_bytes, self._held_bytes())
-                return c, self._take(same[:n], c)
+                victims, self._closing = self._closing, []
+                return c, self._take(same[:n], c), victims
             n = n // 2
         if best is not None:
-            return best, self._take(same[:best.nshots], best)
+            return best, self._take(same[:best.nshots], best), []
         return None
 
     def _take(self, cand, ctx):
@@ -324,7 +347,9 @@ class ShotServer:
 
     def _make_room(self, need: int, keep=None) -> bool:
         """Evict idle contexts (least recently used first, `keep` last) until
-        `need` more bytes fit in the budget."""
+        `need` more bytes fit in the budget.  Their handles are released
+        outside the scheduler's lock (a device free waits for the device):
+        by the thread of the batch that needed the room, else by the loop."""
         if need > self.budget:
             return False
         while self._held_bytes() + need > self.budget:
@@ -336,14 +361,19 @@ class ShotServer:
                     return False
             victim = min(idle, key=lambda c: c.last_used)
             self._pool.remove(victim)
-            self.backend.close(victim.handle)
+            self._closing.append(victim.handle)
         return True
 
     # -- execution --------------------------------------------------------------
-    def _run_batch(self, ctx: _Context, batch):
+    def _run_batch(self, ctx: _Context, batch, victims=()):
         reqs = [r for r, _ in batch]
         t_start = time.perf_counter()
         try:
+            for h in victims:
+                self.backend.close(h)
+            if ctx.handle is None:
+                p, kind, n, mm, ms, mr, fmt, model = ctx.spec
+                ctx.handle = self.backend.create(p, kind, n, mm, ms, mr, fmt, model=model)
             midx = []
             for r in reqs:
                 mk = _model_key(r)
@@ -377,7 +407,8 @@ class ShotServer:
                 if ctx in self._pool:
                     self._pool.remove(ctx)
             try:
-                self.backend.close(ctx.handle)
+                if ctx.handle is not None:
+                    self.backend.close(ctx.handle)
             except Exception:
                 pass
         finally:

@@ -45,6 +45,20 @@ def make_params(p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=
     return c
 
 
+def opt_step(l2t, epst, fp64: bool = True) -> float:
+    """Step length of the line search from the misfits ``l2t`` of the three
+    test steps ``epst`` (src/calc_opt_step.c): the extremum of the fitted
+    parabola with the reference's clamps, solved in double (``fp64``) or in
+    the reference's float arithmetic."""
+    a = np.ascontiguousarray(l2t, np.float32)[:3]
+    e = np.ascontiguousarray(epst, np.float32)[:3]
+    out = C.c_float()
+    rc = _lib.load().ifos_opt_step(_fp(a), _fp(e), 1 if fp64 else 0, C.byref(out))
+    if rc != 0:
+        raise IfosError(rc, "ifos_opt_step")
+    return out.value
+
+
 class ShotSolver:
     """One device context: ``max_shots`` shot slots stepped together."""
 

@@ -250,6 +250,17 @@ enum {
 int ifos_set_option(ifos_ctx *ctx, int option, int value);
 int ifos_get_option(const ifos_ctx *ctx, int option, int *value);
 
+/* Step length of the line search (src/calc_opt_step.c:73-112, solving with
+ * src/solvelin.c:53-70): fits the parabola a + b*eps + c*eps^2 through the
+ * misfits l2t[0..2] of the test steps epst[0..2] by Gaussian elimination
+ * without pivoting and returns its extremum -b/(2c) in *opteps, clamped as
+ * the reference clamps it (epst[2] when the parabola opens downward with
+ * l2t[1] > l2t[2] or when the extremum lies beyond epst[2]; epst[0] when it
+ * is negative).  fp64 = 1 solves in double (this library's line search);
+ * fp64 = 0 in float with the reference's operation order, bit-identical to
+ * it.  Host code: needs no context or device. */
+int ifos_opt_step(const float *l2t, const float *epst, int fp64, float *opteps);
+
 /* FP64 dot product without any device allocation.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc (code running in
  * host callbacks or latency-bound loops where an allocation would stall, or

@@ -48,7 +48,7 @@ class FakeBackend:
         per = p.nx * p.ny * p.nt // 1000 if kind == GRADIENT else p.nx * p.ny // 100
         return 10 + n * per
 
-    def create(self, p, kind, n, max_models, max_src, max_rec, snap_format):
+    def create(self, p, kind, n, max_models, max_src, max_rec, snap_format, model=None):
         nb = self.bytes_needed(p, kind, n, max_models, max_src, max_rec, snap_format)
         with self.lock:
             self.live += nb
