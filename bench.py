@@ -60,6 +60,8 @@ def parse():
                     help="snapshot format of the batched form (the plain FP32 path always stores fp32)")
     ap.add_argument("--batch", type=int, default=0, help="shots per context (0: chosen by the autotuner)")
     ap.add_argument("--max-batch", type=int, default=8)
+    ap.add_argument("--opts", default=None,
+                    help='execution options as JSON (e.g. \'{"pdl": 0, "tile_order": 1}\'); default: autotuned')
     ap.add_argument("--nt", type=int, default=6000, help="time steps (6000 is the workload; smaller only for tests)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -510,6 +512,7 @@ def main():
 
     from ifos_b200 import autotune as A
     from ifos_b200 import workloads as W
+    from ifos_b200.multigpu import shot_index
     from ifos_b200.solver import ShotSolver
 
     p, model, geoms = workload(args.nt)
@@ -518,7 +521,7 @@ def main():
     sigs = {}
 
     def shot(k):
-        idx = (rank + world * k) % len(geoms)
+        idx = shot_index(k, rank, world, len(geoms))
         g = geoms[idx]
         if idx not in sigs:
             sigs[idx] = W.ricker(p, g.srcpos)
@@ -527,11 +530,12 @@ def main():
     # ---- the plain FP32 path (drop-in form), for the speed-up of the batched form ----
     plain = None
     if not args.no_plain:
-        plain = plain_path(p, [model], [(0, geoms[(rank + world * k) % len(geoms)]) for k in range(3)], device)
+        plain = plain_path(p, [model], [(0, geoms[shot_index(k, rank, world, len(geoms))]) for k in range(3)], device)
 
     # ---- the batched, low-precision-snapshot form: batch size and options tuned ----
     if args.batch > 0:
-        B, opts = args.batch, A.tune(p, model, args.batch, args.snap, device)
+        B = args.batch
+        opts = json.loads(args.opts) if args.opts else A.tune(p, model, args.batch, args.snap, device)
     else:
         free = torch.cuda.mem_get_info(device)[0]
         choice = A.best_batch(p, model, int(free * 0.85), max_batch=args.max_batch, snap_format=args.snap,

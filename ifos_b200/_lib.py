@@ -104,7 +104,7 @@ def load():
                                        C.POINTER(C.c_ubyte)]),
         "ifos_set_option": (C.c_int, [vp, C.c_int, C.c_int]),
         "ifos_get_option": (C.c_int, [vp, C.c_int, IP]),
-        "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, DP, DP]),
+        "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, IP, DP, DP]),
         "ifos_fetch_snapshot": (C.c_int, [vp, C.c_int, C.c_int, FP]),
         "ifos_opt_step": (C.c_int, [FP, FP, C.c_int, FP]),
     }

@@ -525,11 +525,15 @@ __device__ __forceinline__ float seg_absmax_warp(float v0, float v1, bool ok0, b
     const unsigned a1 = ok1 ? (__float_as_uint(v1) & 0x7fffffffu) : 0u;
     return __uint_as_float(__reduce_max_sync(0xffffffffu, a0 > a1 ? a0 : a1));
 }
-// the quantisation factor q and the stored read-back scale of a segment maximum m
+// The quantisation factor q and the stored read-back scale inv of a segment
+// maximum m.  Neither needs to be correctly rounded: q * inv = 1 within a few
+// ulps of fp32 (far below fp16's 2^-11) and m * q stays below 65504, so the
+// fast approximate division (a reciprocal and a multiply) serves; it is exact
+// enough for m below 2^126 (a wavefield amplitude of 8.5e37).
 __device__ __forceinline__ void seg_scales(float m, float &q, float &inv) {
     if (m >= 1e-30f) {
-        q = kSegTop / m;
-        inv = m / kSegTop;
+        q = __fdividef(kSegTop, m);
+        inv = m * (1.0f / kSegTop);
     } else {
         q = 0.0f;
         inv = 0.0f;

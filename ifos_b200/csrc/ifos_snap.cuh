@@ -431,9 +431,14 @@ __global__ void k_dot_final(const double *partial, int nb, double *out) {
 // per trace, running float sums times DT, time-reversed difference; the
 // misfit and energy partial sums per trace in double
 __global__ void k_calc_res(const float *obs, const float *syn, float *diff, int ntr, int ns, float dt,
-                           double *l2_tr, double *en_tr) {
+                           double *l2_tr, double *en_tr, const int *kill = nullptr) {
     const int tr = blockIdx.x * blockDim.x + threadIdx.x;
     if (tr >= ntr) return;
+    if (kill && kill[tr]) {  // a killed trace keeps a zero residual and adds nothing (src/calc_res.c:196-197)
+        l2_tr[tr] = 0.0;
+        en_tr[tr] = 0.0;
+        return;
+    }
     const float *s = syn + (long long)tr * ns, *d = obs + (long long)tr * ns;
     float *df = diff + (long long)tr * ns;
     float rs = 0.0f, rd = 0.0f;

@@ -1512,7 +1512,8 @@ extern "C" int ifos_calc_res(ifos_ctx *c, int ntr, const float *obs, const float
 // component the residual of calc_res (src/calc_res.c, LNORM=2) is written
 // time-reversed into the staged adjoint sources, and the FP64 misfit and
 // energy are summed per slot.
-extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, double *l2, double *energy) {
+extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, const int *kill, double *l2,
+                                     double *energy) {
     if (!c || !obs) return IFOS_ERR_ARG;
     if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
     if (c->fwd_nshots < nshots) return fail(c, IFOS_ERR_STATE, "no forward seismograms for these slots");
@@ -1530,11 +1531,14 @@ extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, 
     }
     const size_t comp = (size_t)mr * ns, obs_bytes = (size_t)nshots * 3 * comp * 4;
     const size_t tb = (size_t)nshots * 3 * mr * 2 * sizeof(double);
+    const size_t kb = kill ? ((size_t)nshots * mr * sizeof(int) + 255) / 256 * 256 : 0;
     void *scr = nullptr;
-    if (int rc = scratch(c, tb + obs_bytes, &scr)) return rc;
+    if (int rc = scratch(c, tb + kb + obs_bytes, &scr)) return rc;
     double *tr = (double *)scr;
-    float *d_obs = (float *)((char *)scr + tb);
+    int *d_kill = kill ? (int *)((char *)scr + tb) : nullptr;
+    float *d_obs = (float *)((char *)scr + tb + kb);
     CK(cudaMemcpyAsync(d_obs, obs, obs_bytes, cudaMemcpyHostToDevice, c->st));
+    if (kill) CK(cudaMemcpyAsync(d_kill, kill, (size_t)nshots * mr * sizeof(int), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemsetAsync(c->adj.p, 0, obs_bytes, c->st));
     CK(cudaMemsetAsync(tr, 0, tb, c->st));
     for (int s = 0; s < nshots; s++) {
@@ -1546,7 +1550,7 @@ extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, 
             float *adj = (float *)c->adj.p + ((size_t)s * 3 + k) * comp;
             double *t = tr + ((size_t)s * 3 + k) * mr * 2;
             k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>(d_obs + ((size_t)s * 3 + k) * comp, syn, adj, ntr, ns,
-                                                             p.dt, t, t + mr);
+                                                             p.dt, t, t + mr, d_kill ? d_kill + (size_t)s * mr : nullptr);
             c->launches++;
         }
     }

@@ -192,19 +192,26 @@ class ShotSolver:
                                            C.byref(en)))
         return diff, l2.value, en.value
 
-    def residual_adjoint(self, obs, nshots: int = 1):
+    def residual_adjoint(self, obs, nshots: int = 1, kill=None):
         """Residuals of slots [0, nshots) of the last forward run against the
         observed seismograms ``obs`` (nshots, 3, max_rec, NT; vx, vy,
         vz-or-p), staged as the adjoint sources of the next ``adjoint(None,
-        nshots)``.  Returns the per-slot FP64 (misfit, energy) arrays."""
+        nshots)``; ``kill`` (nshots, max_rec) marks killed traces.  Returns
+        the per-slot FP64 (misfit, energy) arrays."""
         obs = _f32(obs)
         want = (nshots, 3, self.max_rec, self.p.nt)
         if obs.shape != want:
             raise ValueError(f"observed seismograms must be {want}, got {obs.shape}")
+        kp = None
+        if kill is not None:
+            kill = np.ascontiguousarray(kill, np.int32)
+            if kill.shape != (nshots, self.max_rec):
+                raise ValueError(f"kill must be {(nshots, self.max_rec)}, got {kill.shape}")
+            kp = kill.ctypes.data_as(C.POINTER(C.c_int))
         l2 = np.zeros(nshots, np.float64)
         en = np.zeros(nshots, np.float64)
         DP = C.POINTER(C.c_double)
-        self._check(self.lib.ifos_residual_adjoint(self._ctx, int(nshots), _fp(obs), l2.ctypes.data_as(DP),
+        self._check(self.lib.ifos_residual_adjoint(self._ctx, int(nshots), _fp(obs), kp, l2.ctypes.data_as(DP),
                                                    en.ctypes.data_as(DP)))
         return l2, en
 

@@ -180,8 +180,12 @@ int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, fl
  * observed seismograms `obs` (slot x 3 x max_rec x NT, host; components
  * vx, vy, vz-or-p) on the device, stages them as the adjoint sources of the
  * next ifos_adjoint(ctx, nshots, NULL, ...) and returns each slot's FP64
- * misfit and energy in l2[nshots] / energy[nshots] (either may be NULL). */
-int ifos_residual_adjoint(ifos_ctx *ctx, int nshots, const float *obs, double *l2, double *energy);
+ * misfit and energy in l2[nshots] / energy[nshots] (either may be NULL).
+ * kill (slot x max_rec ints, or NULL) marks traces killed for this shot (a
+ * column of the trace-kill table): they keep a zero residual and add nothing
+ * to the sums, as calc_res skips them (src/calc_res.c:196-197). */
+int ifos_residual_adjoint(ifos_ctx *ctx, int nshots, const float *obs, const int *kill, double *l2,
+                          double *energy);
 
 /* Offset-based trace-kill table (src/create_trkill_table.c:21-46), on the
  * device and bit-identical to the reference: killtable (ntr_glob x nsrc_glob,
