@@ -110,18 +110,27 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
+def ncu_traffic(shots):
     """DRAM bytes per launch of the stress kernel from the committed ncu
-    summary (profiles/ncu_traffic.txt: `stress_visco_fp32 <bytes> <cells>`),
-    scaled to this grid by cells."""
+    summaries (profiles/ncu_traffic.txt: `stress_visco_fp32 <bytes> <cells>
+    <shots per launch>`): the capture with the same shots per launch, else
+    the single-shot capture scaled by shots.  Returns (bytes for one launch
+    of `cells`-cell shots, note)."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    rows = []
     try:
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 3 and parts[0] == "stress_visco_fp32":
-                return float(parts[1]), float(parts[2])
+            if len(parts) >= 4 and parts[0] == "stress_visco_fp32":
+                rows.append((float(parts[1]), float(parts[2]), int(parts[3])))
     except OSError:
         pass
+    for b, c, s in rows:
+        if s == shots:
+            return b, c, f"ncu capture of a {s}-shot launch"
+    for b, c, s in rows:
+        if s == 1:
+            return b * shots, c, f"ncu capture of a 1-shot launch, scaled by {shots} shots"
     return None
 
 
@@ -634,14 +643,14 @@ def main():
     avg_s = s_ms / max(1, s_n)
     b_s = stress_bytes(p) * B  # one launch steps all B slots
     achieved = b_s / (avg_s / 1000.0) / 1e9 if s_n else None
-    tr = ncu_traffic()
-    traffic = tr[0] * cells * B / tr[1] if tr else None
+    tr = ncu_traffic(B)
+    traffic = tr[0] * cells / tr[1] if tr else None
     roof = {"kernel": f"viscoelastic stress update (L=3 memory variables + CPML), fp32, {B} shot(s) per launch",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
             "fallback 6650 GB/s",
-            "traffic": traffic, "traffic_source": "ncu capture of one single-shot launch, scaled by cells x shots",
+            "traffic": traffic, "traffic_source": (tr[2] + ", scaled to this grid by cells") if tr else None,
             "alg_bytes_per_launch": b_s, "avg_launch_ms": avg_s, "sampled_launches": s_n,
             "velocity_kernel": {"avg_launch_ms": v_ms / max(1, v_n),
                                 "achieved_gbs": B * (velocity_bytes(p, False) + velocity_bytes(p, True)) / 2 /

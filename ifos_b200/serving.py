@@ -96,7 +96,7 @@ def shape_key(req: ShotRequest):
 class GpuBackend:
     """Backend on the CUDA library: one ShotSolver per context."""
 
-    def __init__(self, device: int = 0, tune: bool = True):
+    def __init__(self, device: int = 0, tune: bool = False):
         self.device = device
         self.tune = tune
 
@@ -113,13 +113,17 @@ class GpuBackend:
 
     def create(self, p: ShotParams, kind: str, nshots: int, max_models: int, max_src: int, max_rec: int,
                snap_format: str, model: Optional[dict] = None):
-        """A context for the batch; its execution options come from the
-        autotuner (timed once per shape and batch size, then cached)."""
+        """A context for the batch.  Its execution options are the ones the
+        autotuner picked on the measured workloads (graph replay, no PDL,
+        slot-minor tiles for several shots); with ``tune`` they are timed
+        once per shape (at two shots, then cached) instead."""
         from .solver import ShotSolver
-        opts = {}
+        opts = dict(graphs=1, pdl=0, tile_order=1 if nshots > 1 else 0)
         if self.tune and model is not None and kind == GRADIENT:
             from . import autotune
-            opts = autotune.tune(p, model, nshots, snap_format, self.device)
+            opts = autotune.tune(p, model, 2, snap_format, self.device)
+            if nshots == 1:
+                opts["tile_order"] = 0
         s = ShotSolver(p, max_shots=nshots, max_models=max_models, max_src=max_src, max_rec=max_rec,
                        snapshots=(kind == GRADIENT), snap_format=snap_format, device=self.device)
         if opts:
