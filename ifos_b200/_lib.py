@@ -45,6 +45,11 @@ class IfosParams(C.Structure):
     ]
 
 
+class IfosWindow(C.Structure):
+    _fields_ = [("tw_ind", C.c_int), ("picks", C.POINTER(C.c_float)), ("gamma", C.c_float),
+                ("twl_plus", C.c_float), ("twl_minus", C.c_float)]
+
+
 class IfosError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"ifos error {code}: {msg}")
@@ -104,7 +109,7 @@ def load():
                                        C.POINTER(C.c_ubyte)]),
         "ifos_set_option": (C.c_int, [vp, C.c_int, C.c_int]),
         "ifos_get_option": (C.c_int, [vp, C.c_int, IP]),
-        "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, IP, DP, DP]),
+        "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, IP, C.POINTER(IfosWindow), DP, DP]),
         "ifos_fetch_snapshot": (C.c_int, [vp, C.c_int, C.c_int, FP]),
         "ifos_opt_step": (C.c_int, [FP, FP, C.c_int, FP]),
     }

@@ -37,14 +37,27 @@ def _inputs(sources, header):
     return files
 
 
+def _digest(sources, header, extra=()) -> str:
+    """Hash of every input file and of the flags: a library is current when
+    the stamp written beside it matches (modification times can be fooled by
+    an edit made while a compile is running)."""
+    import hashlib
+    h = hashlib.sha256(" ".join(ARCH + list(extra)).encode())
+    for f in _inputs(sources, header):
+        with open(f, "rb") as fh:
+            h.update(f.encode() + b"\0" + fh.read())
+    return h.hexdigest()
+
+
 def up_to_date(lib=LIB, sources=SOURCES, header="ifos_gpu.h") -> bool:
-    if not os.path.exists(lib):
+    if not os.path.exists(lib) or not os.path.exists(lib + ".stamp"):
         return False
-    t = os.path.getmtime(lib)
-    return all(os.path.getmtime(f) <= t for f in _inputs(sources, header))
+    with open(lib + ".stamp") as fh:
+        return fh.read().strip() == _digest(sources, header)
 
 
-def _compile(lib, sources, verbose, extra):
+def _compile(lib, sources, verbose, extra, header="ifos_gpu.h"):
+    stamp = _digest(sources, header) if not extra else None
     cmd = [nvcc(), "-O3", *ARCH, "-lineinfo", "--fmad=false", "-std=c++17", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
            "-o", lib + ".tmp", *[os.path.join(CSRC, s) for s in sources], "-lcudart", *extra]
@@ -52,6 +65,11 @@ def _compile(lib, sources, verbose, extra):
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(lib + ".tmp", lib)
+    if stamp:
+        with open(lib + ".stamp", "w") as fh:
+            fh.write(stamp + "\n")
+    elif os.path.exists(lib + ".stamp"):
+        os.remove(lib + ".stamp")  # built with extra flags: not the default build
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
@@ -60,7 +78,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if force or not up_to_date():
         _compile(LIB, SOURCES, verbose, extra)
     if force or not up_to_date(LIB_COMPAT, SOURCES_COMPAT, "ifos_compat.h"):
-        _compile(LIB_COMPAT, SOURCES_COMPAT, verbose, extra)
+        _compile(LIB_COMPAT, SOURCES_COMPAT, verbose, extra, "ifos_compat.h")
     return LIB
 
 

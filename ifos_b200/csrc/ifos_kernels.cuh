@@ -114,12 +114,16 @@ __device__ __forceinline__ T tap(int m, T s, T t, bool z0 = false) {
     return (m == 1 && !z0) ? t : s + t;
 }
 
-// CPML recursion of every kernel: psi = b*psi + a*d; d = d/K + psi
+// CPML recursion of every kernel: psi = b*psi + a*d; d = d/K + psi.  With
+// every K equal to 1 (k_one) the quotient is d itself, and the division is
+// not issued at all: an IEEE division of a zero or tiny d (the strips before
+// the wavefield reaches them) takes its slow path.
 template <typename T>
 __device__ inline T cpml(T *psi, T b, T a, T K, T d, int k_one = 0) {
-    T ps = b * *psi + a * d;
+    const T ps = b * *psi + a * d;
     *psi = ps;
-    return (k_one ? d : d / K) + ps;
+    if (k_one) return d + ps;
+    return d / K + ps;
 }
 
 // CPML on precomputed strip indices (0: not in the strip): hx is the 1-based

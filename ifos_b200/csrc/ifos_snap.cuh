@@ -430,8 +430,72 @@ __global__ void k_dot_final(const double *partial, int nb, double *out) {
 // residuals of one component, LNORM=2, VELOCITY=0 (src/calc_res.c:137-281):
 // per trace, running float sums times DT, time-reversed difference; the
 // misfit and energy partial sums per trace in double
+// The time window of src/time_window.c:135-210 on one sample: v at 1-based
+// sample j (j >= 2) of trace i, picks [np][ntr]; returns the windowed value
+// and the taper bits (1/2 late/early of the first window, 4/8 of the second).
+__device__ __forceinline__ float tw_sample(float v, int j, int i, int ntr, int tw_ind, const float *picks, float dt,
+                                          float gamma, float twl_plus, float twl_minus, unsigned char &m) {
+    const float time = (float)(j * dt);
+    m = 0;
+    float p1, l1, l2;
+    if (tw_ind == 1 || tw_ind == 2) {
+        p1 = picks[i];
+        l1 = picks[ntr + i];
+        l2 = picks[2 * ntr + i];
+    } else {
+        p1 = picks[i];
+        l1 = twl_plus;
+        l2 = twl_minus;
+    }
+    const float dumpa = (time - p1 - l1);
+    const float taper = (float)exp((double)(-gamma * dumpa));
+    const float dumpb = (time - p1 + l2);
+    const float taper1 = (float)exp((double)(-gamma * dumpb));
+    if (tw_ind != 2) {
+        if (time >= p1 + l1) {
+            v = v * taper;
+            m |= 1;
+        }
+        if (time <= p1 - l2) {
+            v = v * taper1;
+            m |= 2;
+        }
+        return v;
+    }
+    float dummy = v;
+    if (time >= p1 + l1) {
+        dummy = v * taper;
+        m |= 1;
+    }
+    if (time <= p1 - l2) {
+        dummy = v * taper1;
+        m |= 2;
+    }
+    const float p4 = picks[3 * ntr + i], l5 = picks[4 * ntr + i], l6 = picks[5 * ntr + i];
+    const float dumpc = (time - p4 - l5);
+    const float taper2 = (float)exp((double)(-gamma * dumpc));
+    const float dumpd = (time - p4 + l6);
+    const float taper3 = (float)exp((double)(-gamma * dumpd));
+    if (time >= p4 + l5) {
+        v = v * taper2;
+        m |= 4;
+    }
+    if (time <= p4 - l6) {
+        v = v * taper3;
+        m |= 8;
+    }
+    return v + dummy;
+}
+
+// time window of the residual step (TIMEWIN=1): picks [np][ntr] of one shot
+struct KWindow {
+    const float *picks;  // NULL: no window
+    int stride;          // traces between the pick rows
+    int tw_ind;
+    float gamma, twl_plus, twl_minus;
+};
 __global__ void k_calc_res(const float *obs, const float *syn, float *diff, int ntr, int ns, float dt,
-                           double *l2_tr, double *en_tr, const int *kill = nullptr) {
+                           double *l2_tr, double *en_tr, const int *kill = nullptr, KWindow win = KWindow{}) {
     const int tr = blockIdx.x * blockDim.x + threadIdx.x;
     if (tr >= ntr) return;
     if (kill && kill[tr]) {  // a killed trace keeps a zero residual and adds nothing (src/calc_res.c:196-197)
@@ -446,7 +510,14 @@ __global__ void k_calc_res(const float *obs, const float *syn, float *diff, int 
     for (int j = 0; j < ns; j++) {
         rs += s[j];
         rd += d[j];
-        const float is = rs * dt, id = rd * dt;
+        float is = rs * dt, id = rd * dt;
+        if (win.picks && j >= 1) {  // windowed after the integration (src/calc_res.c:157-160)
+            unsigned char m;
+            is = tw_sample(is, j + 1, tr, win.stride, win.tw_ind, win.picks, dt, win.gamma, win.twl_plus,
+                           win.twl_minus, m);
+            id = tw_sample(id, j + 1, tr, win.stride, win.tw_ind, win.picks, dt, win.gamma, win.twl_plus,
+                           win.twl_minus, m);
+        }
         const float r = is - id;
         df[ns - 1 - j] = r;
         l2 += (double)r * (double)r;
@@ -485,58 +556,8 @@ __global__ void k_time_window(float *sec, int ntr, int ns, int tw_ind, const flo
         if (mask) mask[k] = 0;
         return;
     }
-    const float time = (float)(j * dt);
-    float v = sec[k];
-    unsigned char m = 0;
-    float p1, l1, l2;
-    if (tw_ind == 1 || tw_ind == 2) {
-        p1 = picks[i];
-        l1 = picks[ntr + i];
-        l2 = picks[2 * ntr + i];
-    } else {
-        p1 = picks[i];
-        l1 = twl_plus;
-        l2 = twl_minus;
-    }
-    const float dumpa = (time - p1 - l1);
-    const float taper = (float)exp((double)(-gamma * dumpa));
-    const float dumpb = (time - p1 + l2);
-    const float taper1 = (float)exp((double)(-gamma * dumpb));
-    if (tw_ind != 2) {
-        if (time >= p1 + l1) {
-            v = v * taper;
-            m |= 1;
-        }
-        if (time <= p1 - l2) {
-            v = v * taper1;
-            m |= 2;
-        }
-    } else {
-        float dummy = v;
-        if (time >= p1 + l1) {
-            dummy = v * taper;
-            m |= 1;
-        }
-        if (time <= p1 - l2) {
-            dummy = v * taper1;
-            m |= 2;
-        }
-        const float p4 = picks[3 * ntr + i], l5 = picks[4 * ntr + i], l6 = picks[5 * ntr + i];
-        const float dumpc = (time - p4 - l5);
-        const float taper2 = (float)exp((double)(-gamma * dumpc));
-        const float dumpd = (time - p4 + l6);
-        const float taper3 = (float)exp((double)(-gamma * dumpd));
-        if (time >= p4 + l5) {
-            v = v * taper2;
-            m |= 4;
-        }
-        if (time <= p4 - l6) {
-            v = v * taper3;
-            m |= 8;
-        }
-        v = v + dummy;
-    }
-    sec[k] = v;
+    unsigned char m;
+    sec[k] = tw_sample(sec[k], j, i, ntr, tw_ind, picks, dt, gamma, twl_plus, twl_minus, m);
     if (mask) mask[k] = m;
 }
 

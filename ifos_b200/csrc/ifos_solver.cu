@@ -26,6 +26,11 @@ using namespace ifos;
 #define IFOS_TILE_Y 8
 #endif
 static constexpr int kTileY = IFOS_TILE_Y;
+// rows of the velocity ops' tiles (their own tensor maps when they differ)
+#ifndef IFOS_VTILE_Y
+#define IFOS_VTILE_Y 8
+#endif
+static constexpr int kTileYV = IFOS_VTILE_Y;
 
 // Stages of an op's shared-memory ring: as many as fit when kRingBlocks
 // blocks share an SM's 227 KB (2..6).  Loads stay in flight in every stage
@@ -34,9 +39,9 @@ static constexpr int kTileY = IFOS_TILE_Y;
 #define IFOS_RING_BLOCKS 3
 #endif
 constexpr int kRingBlocks = IFOS_RING_BLOCKS;
-template <int FD, int NH, int NP, int NO>
+template <int FD, int NH, int NP, int NO, int TY = kTileY>
 constexpr int ring_stages() {
-    constexpr size_t stage = Pipe<FD, kTileY, NH, NP, NO, 1>::bytes();
+    constexpr size_t stage = Pipe<FD, TY, NH, NP, NO, 1>::bytes();
     constexpr int n = (int)((232448 / kRingBlocks - 1024) / stage);
     return n < 2 ? 2 : (n > 6 ? 6 : n);
 }
@@ -131,6 +136,7 @@ struct ifos_ctx {
     bool fused_snap = false;  // fp32 snapshots written by the stencil kernels
     bool pdl = true;          // time-loop kernels launched as programmatic dependents
     KMaps maps{};
+    KMaps maps_v{};  // tensor maps of the velocity ops' tile height
     KTma ktma{};
     int num_sms = 148;
     // execution options (IFOS_OPT_*)
@@ -409,6 +415,12 @@ static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     if (!encode_planes(&c->maps.halo, c->state.p, L.pitch, L.rows, st_planes, kTileX + 2 * xh, kTileY + 2 * fdoh) ||
         !encode_planes(&c->maps.plain, c->state.p, L.pitch, L.rows, st_planes, kTileX, kTileY) ||
         !encode_planes(&c->maps.model, c->models.p, L.pitch, L.rows, md_planes, kTileX, kTileY))
+        return;
+    c->maps_v = c->maps;
+    if (kTileYV != kTileY &&
+        (!encode_planes(&c->maps_v.halo, c->state.p, L.pitch, L.rows, st_planes, kTileX + 2 * xh, kTileYV + 2 * fdoh) ||
+         !encode_planes(&c->maps_v.plain, c->state.p, L.pitch, L.rows, st_planes, kTileX, kTileYV) ||
+         !encode_planes(&c->maps_v.model, c->models.p, L.pitch, L.rows, md_planes, kTileX, kTileYV)))
         return;
     // fp32 snapshots are written by the stencil kernels themselves
     t.snap_ntd = c->p.nt / c->p.dtinv;
@@ -874,10 +886,11 @@ struct Launcher {
             occ[d] = o > 0 ? o : 1;
         }
         const long long ntiles =
-            (long long)((c->p.nx + kTileX - 1) / kTileX) * ((c->p.ny + kTileY - 1) / kTileY) * nshots;
+            (long long)((c->p.nx + kTileX - 1) / kTileX) * ((c->p.ny + P::TILE_Y - 1) / P::TILE_Y) * nshots;
         const int bps = c->blocks_per_sm > 0 ? std::min(c->blocks_per_sm, occ[d]) : occ[d];
         const int grid = (int)std::min<long long>(ntiles, (long long)bps * c->num_sms);
-        launch_dep(c->st, c->pdl, kern, dim3(grid), dim3(32, kComputeWarps + 1), P::bytes(), c->maps, op, nshots,
+        const KMaps &mp = P::TILE_Y == kTileY ? c->maps : c->maps_v;
+        launch_dep(c->st, c->pdl, kern, dim3(grid), dim3(32, kComputeWarps + 1), P::bytes(), mp, op, nshots,
                    (int *)c->bad.p);
     }
     // the snapshot a launch stores (hin < 0: none)
@@ -900,12 +913,12 @@ struct Launcher {
         const KTma &t = c->ktma;
         if (c->ac) {
             constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
-            pipelined(OpVPsv<FD, kTileY, ring_stages<FD, 1, NP, 0>(), Q, SW, P1, true>{g, S, M, t, snap_out(hin)});
+            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 1, NP, 0, kTileYV>(), Q, SW, P1, true>{g, S, M, t, snap_out(hin)});
             return;
         }
         if (c->psv) {
             constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
-            pipelined(OpVPsv<FD, kTileY, ring_stages<FD, 3, NP, 0>(), Q, SW, P1, false>{g, S, M, t, snap_out(hin)});
+            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 3, NP, 0, kTileYV>(), Q, SW, P1, false>{g, S, M, t, snap_out(hin)});
         }
     }
     // hin: snapshot index stored by this step's kernels (-1 none)
@@ -923,7 +936,7 @@ struct Launcher {
             else if (want_p1) v_one<FD, false, 0, true>(hin);
             else v_one<FD, false, 0, false>(-1);
         }
-        if (c->sh) pipelined(OpVSh<FD, kTileY, ring_stages<FD, 2, 2, 0>()>{c->g, S, M, c->ktma, snap_out(hin)});
+        if (c->sh) pipelined(OpVSh<FD, kTileYV, ring_stages<FD, 2, 2, 0, kTileYV>()>{c->g, S, M, c->ktma, snap_out(hin)});
     }
     template <int FD, int LL>
     void s_visc_pipe(int hin) {
@@ -1512,8 +1525,8 @@ extern "C" int ifos_calc_res(ifos_ctx *c, int ntr, const float *obs, const float
 // component the residual of calc_res (src/calc_res.c, LNORM=2) is written
 // time-reversed into the staged adjoint sources, and the FP64 misfit and
 // energy are summed per slot.
-extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, const int *kill, double *l2,
-                                     double *energy) {
+extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, const int *kill,
+                                     const ifos_window *win, double *l2, double *energy) {
     if (!c || !obs) return IFOS_ERR_ARG;
     if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
     if (c->fwd_nshots < nshots) return fail(c, IFOS_ERR_STATE, "no forward seismograms for these slots");
@@ -1532,13 +1545,23 @@ extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, 
     const size_t comp = (size_t)mr * ns, obs_bytes = (size_t)nshots * 3 * comp * 4;
     const size_t tb = (size_t)nshots * 3 * mr * 2 * sizeof(double);
     const size_t kb = kill ? ((size_t)nshots * mr * sizeof(int) + 255) / 256 * 256 : 0;
+    int np = 0;
+    if (win) {
+        if (!win->picks || win->tw_ind < 0 || win->tw_ind > 2) return fail(c, IFOS_ERR_ARG, "bad time window");
+        np = win->tw_ind == 0 ? 1 : (win->tw_ind == 1 ? 3 : 6);
+    }
+    const size_t pb = ((size_t)nshots * np * mr * sizeof(float) + 255) / 256 * 256;
     void *scr = nullptr;
-    if (int rc = scratch(c, tb + kb + obs_bytes, &scr)) return rc;
+    if (int rc = scratch(c, tb + kb + pb + obs_bytes, &scr)) return rc;
     double *tr = (double *)scr;
     int *d_kill = kill ? (int *)((char *)scr + tb) : nullptr;
-    float *d_obs = (float *)((char *)scr + tb + kb);
+    float *d_picks = win ? (float *)((char *)scr + tb + kb) : nullptr;
+    float *d_obs = (float *)((char *)scr + tb + kb + pb);
     CK(cudaMemcpyAsync(d_obs, obs, obs_bytes, cudaMemcpyHostToDevice, c->st));
     if (kill) CK(cudaMemcpyAsync(d_kill, kill, (size_t)nshots * mr * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    if (win)
+        CK(cudaMemcpyAsync(d_picks, win->picks, (size_t)nshots * np * mr * sizeof(float), cudaMemcpyHostToDevice,
+                           c->st));
     CK(cudaMemsetAsync(c->adj.p, 0, obs_bytes, c->st));
     CK(cudaMemsetAsync(tr, 0, tb, c->st));
     for (int s = 0; s < nshots; s++) {
@@ -1549,8 +1572,18 @@ extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, 
             const float *syn = (const float *)c->sec.p + ((size_t)s * IFOS_NS + plane[k]) * comp;
             float *adj = (float *)c->adj.p + ((size_t)s * 3 + k) * comp;
             double *t = tr + ((size_t)s * 3 + k) * mr * 2;
+            KWindow kw{};
+            if (win) {
+                kw.picks = d_picks + (size_t)s * np * mr;
+                kw.stride = mr;
+                kw.tw_ind = win->tw_ind;
+                kw.gamma = win->gamma;
+                kw.twl_plus = win->twl_plus;
+                kw.twl_minus = win->twl_minus;
+            }
             k_calc_res<<<(ntr + 127) / 128, 128, 0, c->st>>>(d_obs + ((size_t)s * 3 + k) * comp, syn, adj, ntr, ns,
-                                                             p.dt, t, t + mr, d_kill ? d_kill + (size_t)s * mr : nullptr);
+                                                             p.dt, t, t + mr, d_kill ? d_kill + (size_t)s * mr : nullptr,
+                                                             kw);
             c->launches++;
         }
     }

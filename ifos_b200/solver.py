@@ -192,12 +192,14 @@ class ShotSolver:
                                            C.byref(en)))
         return diff, l2.value, en.value
 
-    def residual_adjoint(self, obs, nshots: int = 1, kill=None):
+    def residual_adjoint(self, obs, nshots: int = 1, kill=None, window=None):
         """Residuals of slots [0, nshots) of the last forward run against the
         observed seismograms ``obs`` (nshots, 3, max_rec, NT; vx, vy,
         vz-or-p), staged as the adjoint sources of the next ``adjoint(None,
-        nshots)``; ``kill`` (nshots, max_rec) marks killed traces.  Returns
-        the per-slot FP64 (misfit, energy) arrays."""
+        nshots)``; ``kill`` (nshots, max_rec) marks killed traces; ``window``
+        = dict(tw_ind, picks (nshots, np, max_rec), gamma, twl_plus,
+        twl_minus) windows the integrated traces first.  Returns the per-slot
+        FP64 (misfit, energy) arrays."""
         obs = _f32(obs)
         want = (nshots, 3, self.max_rec, self.p.nt)
         if obs.shape != want:
@@ -208,10 +210,18 @@ class ShotSolver:
             if kill.shape != (nshots, self.max_rec):
                 raise ValueError(f"kill must be {(nshots, self.max_rec)}, got {kill.shape}")
             kp = kill.ctypes.data_as(C.POINTER(C.c_int))
+        wp = None
+        if window is not None:
+            tw = int(window["tw_ind"])
+            np_ = {0: 1, 1: 3, 2: 6}[tw]
+            picks = np.ascontiguousarray(window["picks"], np.float32).reshape(nshots, np_, self.max_rec)
+            w = _lib.IfosWindow(tw, _fp(picks), float(window.get("gamma", 0.0)), float(window.get("twl_plus", 0.0)),
+                                float(window.get("twl_minus", 0.0)))
+            wp = C.byref(w)
         l2 = np.zeros(nshots, np.float64)
         en = np.zeros(nshots, np.float64)
         DP = C.POINTER(C.c_double)
-        self._check(self.lib.ifos_residual_adjoint(self._ctx, int(nshots), _fp(obs), kp, l2.ctypes.data_as(DP),
+        self._check(self.lib.ifos_residual_adjoint(self._ctx, int(nshots), _fp(obs), kp, wp, l2.ctypes.data_as(DP),
                                                    en.ctypes.data_as(DP)))
         return l2, en
 

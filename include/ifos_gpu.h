@@ -183,9 +183,18 @@ int ifos_calc_res(ifos_ctx *ctx, int ntr, const float *obs, const float *syn, fl
  * misfit and energy in l2[nshots] / energy[nshots] (either may be NULL).
  * kill (slot x max_rec ints, or NULL) marks traces killed for this shot (a
  * column of the trace-kill table): they keep a zero residual and add nothing
- * to the sums, as calc_res skips them (src/calc_res.c:196-197). */
-int ifos_residual_adjoint(ifos_ctx *ctx, int nshots, const float *obs, const int *kill, double *l2,
-                          double *energy);
+ * to the sums, as calc_res skips them (src/calc_res.c:196-197).  win (or
+ * NULL) applies the time windows of TIMEWIN=1 to the integrated synthetic
+ * and observed traces before the residual (src/calc_res.c:157-160), as
+ * ifos_time_window does. */
+typedef struct ifos_window {
+    int tw_ind;          /* TW_IND: 0 one pick + TWLENGTH_PLUS/MINUS, 1 pick + lengths, 2 two windows */
+    const float *picks;  /* host, slot x np x max_rec with np = 1, 3, 6 for tw_ind 0, 1, 2 */
+    float gamma;         /* GAMMA */
+    float twl_plus, twl_minus; /* TWLENGTH_PLUS, TWLENGTH_MINUS (tw_ind 0) */
+} ifos_window;
+int ifos_residual_adjoint(ifos_ctx *ctx, int nshots, const float *obs, const int *kill, const ifos_window *win,
+                          double *l2, double *energy);
 
 /* Offset-based trace-kill table (src/create_trkill_table.c:21-46), on the
  * device and bit-identical to the reference: killtable (ntr_glob x nsrc_glob,

@@ -252,3 +252,45 @@ def test_fp16_segment_snapshots_round_within_half_an_ulp(case):
     bad = np.abs(b - a) > bound
     assert not bad.any(), (int(bad.sum()), np.argwhere(bad)[:5].tolist())
     assert np.abs(a).max() > 0
+
+
+@pytest.mark.parametrize("tw_ind", [0, 2])
+def test_device_residual_with_time_windows(tw_ind):
+    """TIMEWIN=1 inside the device residual: the integrated synthetic and
+    observed traces are windowed (src/time_window.c, applied by
+    src/calc_res.c:157-160) before the residual; equal, bit for bit, to
+    integrating on the host, windowing with ifos_time_window (itself
+    bit-exact against the reference) and staging the difference."""
+    p, model, g, sig, adj = build_case("psv_el_o4")
+    ntr = g.recpos.shape[1]
+    rng = np.random.default_rng(31 + tw_ind)
+    obs = (rng.standard_normal((1, 3, ntr, p.nt)) * 1e-4).astype(np.float32)
+    t_end = p.nt * p.dt
+    pick = rng.uniform(0.2, 0.6, ntr) * t_end
+    lens = [rng.uniform(0.02, 0.1, ntr) * t_end for _ in range(2)]
+    if tw_ind == 0:
+        picks = pick[None, :]
+    else:
+        picks = np.stack([pick, lens[0], lens[1], pick + 0.2 * t_end, lens[1], lens[0]])
+    picks = picks.astype(np.float32)
+    win = dict(tw_ind=tw_ind, picks=picks[None], gamma=20.0 / t_end, twl_plus=0.05 * t_end, twl_minus=0.04 * t_end)
+    with ShotSolver(p, max_rec=ntr) as s:
+        s.upload_model(model)
+        s.setup_shot(0, g.srcpos, sig, g.recpos)
+        sec = s.forward(1, store=True)[0]
+        l2, _ = s.residual_adjoint(obs, 1, window=win)
+        g_dev = s.adjoint(None, 1)[0]
+        want = np.zeros_like(obs)
+        tot = 0.0
+        dt = np.float32(p.dt)
+        for k, plane in ((0, 0), (1, 1)):
+            i_syn = (np.cumsum(sec[plane], axis=1, dtype=np.float32) * dt).astype(np.float32)
+            i_obs = (np.cumsum(obs[0, k], axis=1, dtype=np.float32) * dt).astype(np.float32)
+            w_syn = s.time_window(i_syn, tw_ind, picks, win["gamma"], win["twl_plus"], win["twl_minus"])
+            w_obs = s.time_window(i_obs, tw_ind, picks, win["gamma"], win["twl_plus"], win["twl_minus"])
+            r = (w_syn - w_obs).astype(np.float32)
+            want[0, k] = r[:, ::-1]
+            tot += float(np.sum(r.astype(np.float64) ** 2))
+        g_host = s.adjoint(want, 1)[0]
+    assert bit_equal(g_dev, g_host)
+    assert l2[0] == pytest.approx(tot, rel=1e-12)
