@@ -45,7 +45,7 @@ def _digest(sources, header, extra=()) -> str:
     h = hashlib.sha256(" ".join(ARCH + list(extra)).encode())
     for f in _inputs(sources, header):
         with open(f, "rb") as fh:
-            h.update(f.encode() + b"\0" + fh.read())
+            h.update(os.path.relpath(f, ROOT).encode() + b"\0" + fh.read())
     return h.hexdigest()
 
 

@@ -609,7 +609,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
         // exact shortcuts of the kernels: d/K with K == 1 everywhere, x/DH with DH a power of two
         g.k_one = 1;
         for (int a : {K_X, K_XH, K_Y, K_YH})
-            for (int h = 0; h <= 2 * p.fw; h++)
+            for (int h = 1; h <= 2 * p.fw; h++)  // the profiles are 1-based (index 0 is unused)
                 if (pr.arr[a][h] != 1.0) g.k_one = 0;
         int ex = 0;
         g.dh_pow2 = std::frexp(p.dh, &ex) == 0.5f ? 1 : 0;

@@ -19,6 +19,9 @@ CASES = {
     "sh_visc_o4": dict(wavetype=2, L=2, fl=FL[:2], tau=TAU, f_ref=40.0),
     "acoustic_o4_p": dict(acoustic=1, seismo=2, adjoint_type=4),
     "psv_el_o4_seismo4_force": dict(seismo=4, source_type=3),
+    # CPML with K profiles above 1 (k_max_PML > 1): the d/K division of the recursion
+    "psv_visc_o4_kmax2": dict(L=3, fl=FL, tau=TAU, f_ref=40.0, k_max_pml=2.0),
+    "sh_el_o4_kmax3": dict(wavetype=2, k_max_pml=3.0, free_surf=0),
 }
 
 
