@@ -114,16 +114,29 @@ __device__ __forceinline__ T tap(int m, T s, T t, bool z0 = false) {
     return (m == 1 && !z0) ? t : s + t;
 }
 
+// IEEE round-to-nearest division (what `/` compiles to) that the compiler
+// may not hoist out of the branch it is written in: a speculated division of
+// a zero or tiny dividend (the CPML strips before the wavefield reaches
+// them) takes its slow path even when its result is not used.
+__device__ __forceinline__ float div_rn_pinned(float x, float y) {
+    float q;
+    asm volatile("div.rn.f32 %0, %1, %2;" : "=f"(q) : "f"(x), "f"(y));
+    return q;
+}
+__device__ __forceinline__ double div_rn_pinned(double x, double y) {
+    double q;
+    asm volatile("div.rn.f64 %0, %1, %2;" : "=d"(q) : "d"(x), "d"(y));
+    return q;
+}
+
 // CPML recursion of every kernel: psi = b*psi + a*d; d = d/K + psi.  With
-// every K equal to 1 (k_one) the quotient is d itself, and the division is
-// not issued at all: an IEEE division of a zero or tiny d (the strips before
-// the wavefield reaches them) takes its slow path.
+// every K equal to 1 (k_one) the quotient is d itself and no division runs.
 template <typename T>
 __device__ inline T cpml(T *psi, T b, T a, T K, T d, int k_one = 0) {
     const T ps = b * *psi + a * d;
     *psi = ps;
     if (k_one) return d + ps;
-    return d / K + ps;
+    return div_rn_pinned(d, K) + ps;
 }
 
 // CPML on precomputed strip indices (0: not in the strip): hx is the 1-based
