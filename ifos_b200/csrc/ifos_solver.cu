@@ -39,10 +39,10 @@ static constexpr int kTileYV = IFOS_VTILE_Y;
 #define IFOS_RING_BLOCKS 3
 #endif
 constexpr int kRingBlocks = IFOS_RING_BLOCKS;
-template <int FD, int NH, int NP, int NO, int TY = kTileY>
+template <int FD, int NH, int NP, int NO, int TY = kTileY, int RB = kRingBlocks>
 constexpr int ring_stages() {
     constexpr size_t stage = Pipe<FD, TY, NH, NP, NO, 1>::bytes();
-    constexpr int n = (int)((232448 / kRingBlocks - 1024) / stage);
+    constexpr int n = (int)((232448 / RB - 1024) / stage);
     return n < 2 ? 2 : (n > 6 ? 6 : n);
 }
 
@@ -913,12 +913,12 @@ struct Launcher {
         const KTma &t = c->ktma;
         if (c->ac) {
             constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
-            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 1, NP, 0, kTileYV>(), Q, SW, P1, true>{g, S, M, t, snap_out(hin)});
+            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 1, NP, 0, kTileYV, vblocks(FD)>(), Q, SW, P1, true>{g, S, M, t, snap_out(hin)});
             return;
         }
         if (c->psv) {
             constexpr int NP = (SW == 1 && !Q) ? 6 : 4;
-            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 3, NP, 0, kTileYV>(), Q, SW, P1, false>{g, S, M, t, snap_out(hin)});
+            pipelined(OpVPsv<FD, kTileYV, ring_stages<FD, 3, NP, 0, kTileYV, vblocks(FD)>(), Q, SW, P1, false>{g, S, M, t, snap_out(hin)});
         }
     }
     // hin: snapshot index stored by this step's kernels (-1 none)
@@ -936,7 +936,7 @@ struct Launcher {
             else if (want_p1) v_one<FD, false, 0, true>(hin);
             else v_one<FD, false, 0, false>(-1);
         }
-        if (c->sh) pipelined(OpVSh<FD, kTileYV, ring_stages<FD, 2, 2, 0, kTileYV>()>{c->g, S, M, c->ktma, snap_out(hin)});
+        if (c->sh) pipelined(OpVSh<FD, kTileYV, ring_stages<FD, 2, 2, 0, kTileYV, vblocks(FD)>()>{c->g, S, M, c->ktma, snap_out(hin)});
     }
     template <int FD, int LL>
     void s_visc_pipe(int hin) {
@@ -974,7 +974,7 @@ struct Launcher {
         switch (g.L) {
             case 0:
                 if (c->psv) {
-                    constexpr int NST = ring_stages<FD, 2, 6, 0>();
+                    constexpr int NST = ring_stages<FD, 2, 6, 0, kTileY, sblocks(FD)>();
                     bool done = false;
                     if constexpr (FD >= 5) {
                         if (quirk) {

@@ -39,6 +39,27 @@
 namespace ifos {
 
 constexpr int kComputeWarps = IFOS_NCW;
+// Resident blocks per SM the elastic stress op's launch bounds aim for: four
+// for FDORDER <= 4 (400 x 160 batch of 128: 100-105 vs 109 us per launch),
+// three otherwise.
+constexpr int sblocks(int fdoh) {
+#ifdef IFOS_SBLOCKS
+    return IFOS_SBLOCKS + 0 * fdoh;
+#else
+    return fdoh <= 2 ? 4 : 3;
+#endif
+}
+// Resident blocks per SM the velocity ops' launch bounds aim for.  Four
+// (registers capped at 56, two ring stages) were faster for FDORDER <= 4
+// (400 x 160 batch of 128: 94 vs 103 us per launch), three for the wider
+// stencils (2000 x 600, FDORDER 8, one shot: 22.3 vs 24.6 us).
+constexpr int vblocks(int fdoh) {
+#ifdef IFOS_VBLOCKS
+    return IFOS_VBLOCKS + 0 * fdoh;
+#else
+    return fdoh <= 2 ? 4 : 3;
+#endif
+}
 constexpr int kBlockThreads = 32 * kComputeWarps + 32;
 constexpr int kTileX = 64;
 
@@ -78,7 +99,7 @@ struct KSnapOut {
 };
 
 // NH halo boxes, NP loaded plain boxes, NO output-only plain boxes, NST stages
-template <int FDOH, int TY, int NH, int NP, int NO, int NST>
+template <int FDOH, int TY, int NH, int NP, int NO, int NST, int BCAP = 3>
 struct Pipe {
     static constexpr int TX = kTileX, H = FDOH;
     static constexpr int HE = (FDOH + 1) & ~1;       // x window half width (even)
@@ -92,6 +113,7 @@ struct Pipe {
     static constexpr int TILE_Y = TY;
     static constexpr uint32_t TXB = (uint32_t)((NH * BW * BH + NP * PLS) * 4);
     static constexpr size_t bytes() { return (size_t)NST * STAGE * 4; }
+    static constexpr int BLOCK_CAP = BCAP;  // resident blocks per SM the launch bounds aim for
     static_assert(TY % kComputeWarps == 0, "tile height must be a multiple of the compute warps");
     static_assert(HE <= XH, "x window exceeds the staged halo");
 };
@@ -599,7 +621,7 @@ struct OpSVisc {
 template <int FDOH, int TY, int NST, bool QUIRK>
 struct OpSEl {
     static constexpr int NH_ = 2, NP_ = 6;
-    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST, sblocks(FDOH)>;
     IFOS_OP_MEMBERS
     __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
@@ -694,7 +716,7 @@ template <int FDOH, int TY, int NST, bool QUIRK, int SW, bool P1, bool AC>
 struct OpVPsv {
     static constexpr int NH_ = AC ? 1 : 3;
     static constexpr int NP_ = (SW == 1 && !QUIRK) ? 6 : 4;
-    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST, vblocks(FDOH)>;
     IFOS_OP_MEMBERS
     __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
@@ -839,7 +861,7 @@ struct OpVPsv {
 template <int FDOH, int TY, int NST>
 struct OpVSh {
     static constexpr int NH_ = 2, NP_ = 2;
-    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST, vblocks(FDOH)>;
     IFOS_OP_MEMBERS
     __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
         const int zb = ti.slot * tm.planes_per_slot;
@@ -1098,9 +1120,9 @@ struct OpPAc {
 template <typename P>
 constexpr int ring_blocks() {
     constexpr int by_smem = (int)(232448 / (P::bytes() + 1024));
-    constexpr int by_regs = 65536 / (kBlockThreads * 64);
+    constexpr int by_regs = 65536 / (kBlockThreads * (P::BLOCK_CAP > 3 ? 56 : 64));
     constexpr int b = by_smem < by_regs ? by_smem : by_regs;
-    return b < 1 ? 1 : (b > 3 ? 3 : b);
+    return b < 1 ? 1 : (b > P::BLOCK_CAP ? P::BLOCK_CAP : b);
 }
 
 // the kernel: one Op per launch, persistent over all tiles of all slots
