@@ -550,6 +550,10 @@ def main():
         choice = A.best_batch(p, model, int(free * 0.85), max_batch=args.max_batch, snap_format=args.snap,
                               device=device)
         B, opts = choice["nshots"], choice["options"]
+    if dist:  # every rank runs rank 0's batch size and options (same work per rank)
+        sel = [B, opts]
+        dist.broadcast_object_list(sel, src=0)
+        B, opts = sel
     solver = ShotSolver(p, max_shots=B, max_rec=ntr, snap_format=args.snap, device=device)
     solver.set_options(**opts)
     solver.upload_model(model)
