@@ -299,21 +299,27 @@ def test_device_residual_with_time_windows(tw_ind):
 def test_line_search_batches_the_trial_forwards():
     """The step-length search's trial forwards (3 test models x 3 shots) in
     one batched context give exactly the misfits of separate single-shot
-    runs, and the step is the fit of src/calc_opt_step.c through them."""
+    runs, and the step is the fit of src/calc_opt_step.c through them.  The
+    observed data come from the true model, and the test models are the true
+    model perturbed by (eps - 0.02) x a smooth direction, so the misfit has
+    its minimum near the middle step."""
     from ifos_b200 import linesearch as LS
     from ifos_b200.solver import opt_step
     p, model, g, sig, adj = build_case("psv_el_o4")
     ntr = g.recpos.shape[1]
-    rng = np.random.default_rng(41)
-    direction = rng.standard_normal(model["vp"].shape).astype(np.float32)
+    jj, ii = np.mgrid[0:p.ny, 0:p.nx]
+    direction = (np.exp(-((ii - p.nx / 2) ** 2 + (jj - p.ny / 2) ** 2) / 60.0) * 2.0).astype(np.float32)
     eps = np.array([0.01, 0.02, 0.03], np.float32)
-    models = [{k: (v * (1 + e * 0.5 * direction) if k in ("vp", "vs") else v).astype(np.float32)
+    models = [{k: (v * (1 + (e - 0.02) * direction) if k in ("vp", "vs") else v).astype(np.float32)
                for k, v in model.items()} for e in eps]
     shots, observed = [], []
     for k in range(3):
         src = W.source_rows(p, (12.0 + 15.0 * k) * p.dh, 3 * p.dh, fc=40.0)
         shots.append((src, W.ricker(p, src), g.recpos))
-        observed.append((rng.standard_normal((3, ntr, p.nt)) * 1e-4).astype(np.float32))
+        with ShotSolver(p, max_rec=ntr, snapshots=False) as s:
+            s.upload_model(model)
+            s.setup_shot(0, src, shots[-1][1], g.recpos)
+            observed.append(s.forward(1, store=False)[0][:3].copy())
     step, l2 = LS.step_length(p, models, eps, shots, observed)
     want = np.zeros(3)
     for mi, m in enumerate(models):
@@ -324,4 +330,6 @@ def test_line_search_batches_the_trial_forwards():
                 s.forward(1, store=False, fetch=False)
                 want[mi] += s.residual_adjoint(obs[None], 1)[0][0]
     assert np.array_equal(l2, want)
+    assert l2[1] < l2[0] and l2[1] < l2[2]
     assert step == opt_step(want.astype(np.float32), eps)
+    assert 0.01 < step < 0.03
