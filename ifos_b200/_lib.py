@@ -25,7 +25,7 @@ EXPORTS = [
     "ifos_dot_f64", "ifos_calc_res", "ifos_fd_coeffs", "ifos_cpml_profiles", "ifos_kernel_timing",
     "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_dot_f64_noalloc", "ifos_last_ms", "ifos_launch_count",
     "ifos_sync", "ifos_trkill_table", "ifos_time_window", "ifos_set_option", "ifos_get_option",
-    "ifos_residual_adjoint", "ifos_fetch_snapshot", "ifos_opt_step",
+    "ifos_residual_adjoint", "ifos_fetch_snapshot", "ifos_opt_step", "ifos_timedomain_filt",
 ]
 OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3}
 
@@ -112,6 +112,7 @@ def load():
         "ifos_residual_adjoint": (C.c_int, [vp, C.c_int, FP, IP, C.POINTER(IfosWindow), DP, DP]),
         "ifos_fetch_snapshot": (C.c_int, [vp, C.c_int, C.c_int, FP]),
         "ifos_opt_step": (C.c_int, [FP, FP, C.c_int, FP]),
+        "ifos_timedomain_filt": (C.c_int, [vp, FP, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

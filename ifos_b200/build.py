@@ -74,11 +74,18 @@ def _compile(lib, sources, verbose, extra, header="ifos_gpu.h"):
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     """Build libifos_b200.so (the shot solver) and libifos_compat.so (the
-    reference-named per-kernel entry points); returns the solver library."""
-    if force or not up_to_date():
-        _compile(LIB, SOURCES, verbose, extra)
-    if force or not up_to_date(LIB_COMPAT, SOURCES_COMPAT, "ifos_compat.h"):
-        _compile(LIB_COMPAT, SOURCES_COMPAT, verbose, extra, "ifos_compat.h")
+    reference-named per-kernel entry points); returns the solver library.
+    Concurrent builds (several processes importing the package at once)
+    serialise on a lock file and skip what another one has just built."""
+    import fcntl
+    if not force and up_to_date() and up_to_date(LIB_COMPAT, SOURCES_COMPAT, "ifos_compat.h"):
+        return LIB
+    with open(os.path.join(HERE, ".build.lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        if force or not up_to_date():
+            _compile(LIB, SOURCES, verbose, extra)
+        if force or not up_to_date(LIB_COMPAT, SOURCES_COMPAT, "ifos_compat.h"):
+            _compile(LIB_COMPAT, SOURCES_COMPAT, verbose, extra, "ifos_compat.h")
     return LIB
 
 

@@ -561,4 +561,42 @@ __global__ void k_time_window(float *sec, int ntr, int ns, int tw_ind, const flo
     if (mask) mask[k] = m;
 }
 
+// Butterworth filtering of traces (src/timedomain_filt.c with the vendored
+// libcseife): every trace is one thread's sequential recursion, in double.
+// The reference filters the ns+1 values [0, x_1..x_ns] (its dvector has a
+// zero element before the samples), with each section of the cascade in
+// turn: y_j = f0 x_j + f1 x_{j-1} + f2 x_{j-2} + g1 y_{j-1} + g2 y_{j-2}
+// (contrib/libcseife/cseife_rekfl.c), evaluated left to right.
+struct KIIR {
+    double c[8][5];  // sections: f0 f1 f2 g1 g2
+    int n;
+};
+__global__ void k_butterworth(float *data, double *work, int ntr, int ns, KIIR lp, KIIR hp) {
+    const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tr >= ntr) return;
+    float *d = data + (long long)tr * ns;
+    double *x = work + (long long)tr * (ns + 1);
+    for (int pass = 0; pass < 2; pass++) {
+        const KIIR &f = pass ? hp : lp;
+        if (f.n == 0) continue;
+        x[0] = 0.0;
+        for (int j = 1; j <= ns; j++) x[j] = (double)d[j - 1];
+        // a highpass first subtracts x[0] from every value (contrib/libcseife/cseife.c:156-161); x[0] is 0
+        for (int s = 0; s < f.n; s++) {
+            const double f0 = f.c[s][0], f1 = f.c[s][1], f2 = f.c[s][2], g1 = f.c[s][3], g2 = f.c[s][4];
+            double xa = 0.0, xaa = 0.0, ya = 0.0, yaa = 0.0;
+            for (int j = 0; j <= ns; j++) {
+                const double xn = x[j];
+                const double y = f0 * xn + f1 * xa + f2 * xaa + g1 * ya + g2 * yaa;
+                x[j] = y;
+                xaa = xa;
+                xa = xn;
+                yaa = ya;
+                ya = y;
+            }
+        }
+        for (int j = 1; j <= ns; j++) d[j - 1] = (float)x[j];
+    }
+}
+
 }  // namespace ifos

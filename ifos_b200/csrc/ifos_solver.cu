@@ -1722,6 +1722,78 @@ extern "C" int ifos_opt_step(const float *l2t, const float *epst, int fp64, floa
     return IFOS_OK;
 }
 
+// The cascade of a Butterworth filter of order `m` (contrib/libcseife/
+// cseife.c:164-193 with the section coefficients of cseife_rfk.c): a first-
+// order section when m is odd, then m/2 second-order sections with damping
+// sin(pi/2 (2j-1)/m); t0 = period / sample interval.
+static int butterworth_sections(bool highpass, double t0, int m, KIIR &f) {
+    f.n = 0;
+    if (m < 1 || m / 2 + (m % 2) > 8) return IFOS_ERR_ARG;
+    const double one = 1., two = 2., four = 4., eight = 8.;
+    const double zpi = eight * atan(one);
+    const double eps = zpi / t0;
+    if (m > 2 * (m / 2)) {
+        double *c = f.c[f.n++];
+        c[2] = 0.;
+        c[4] = 0.;
+        c[3] = (two - eps) / (two + eps);
+        if (highpass) {
+            c[0] = two / (two + eps);
+            c[1] = -(c[0]);
+        } else {
+            c[0] = eps / (two + eps);
+            c[1] = c[0];
+        }
+    }
+    const double pih = 2. * atan(1.);
+    for (int j = 1; j <= m / 2; ++j) {
+        const double h = sin(pih * (2 * j - 1) / m);
+        const double epsq = eps * eps;
+        const double a = one - eps * h + epsq / four;
+        const double b = -two + epsq / two;
+        const double cc = one + eps * h + epsq / four;
+        double *c = f.c[f.n++];
+        c[3] = -b / cc;
+        c[4] = -a / cc;
+        if (highpass) {
+            c[0] = one / cc;
+            c[1] = -(c[0]) - c[0];
+        } else {
+            c[0] = epsq / four / cc;
+            c[1] = c[0] + c[0];
+        }
+        c[2] = c[0];
+    }
+    return IFOS_OK;
+}
+
+extern "C" int ifos_timedomain_filt(ifos_ctx *c, float *data, int ntr, int ns, float fc, int order, int method,
+                                    float f_high_pass) {
+    if (!c || !data || ntr < 1 || ns < 1 || (method != 1 && method != 2)) return IFOS_ERR_ARG;
+    if (!(fc > 0.0f) || order < 1) return fail(c, IFOS_ERR_ARG, "corner frequency and order must be positive");
+    CK(cudaSetDevice(c->device));
+    const double dt = (double)c->p.dt;
+    KIIR lp{}, hp{};
+    // src/timedomain_filt.c:53-84: a lowpass at fc (method 1), then a highpass
+    // at F_HIGH_PASS when it is set; method 2 is a highpass at fc
+    if (method == 1 && butterworth_sections(false, (1.0 / (double)fc) / dt, order, lp))
+        return fail(c, IFOS_ERR_ARG, "filter order too high");
+    const double t0_hp = method == 2 ? 1.0 / (double)fc : (f_high_pass != 0.0f ? 1.0 / (double)f_high_pass : 0.0);
+    if ((method == 2 || f_high_pass != 0.0f) && butterworth_sections(true, t0_hp / dt, order, hp))
+        return fail(c, IFOS_ERR_ARG, "filter order too high");
+    const size_t db = (size_t)ntr * ns * 4, wb = (size_t)ntr * (ns + 1) * sizeof(double);
+    void *scr = nullptr;
+    if (int rc = scratch(c, wb + db, &scr)) return rc;
+    double *work = (double *)scr;
+    float *d_data = (float *)((char *)scr + wb);
+    CK(cudaMemcpyAsync(d_data, data, db, cudaMemcpyHostToDevice, c->st));
+    k_butterworth<<<(ntr + 63) / 64, 64, 0, c->st>>>(d_data, work, ntr, ns, lp, hp);
+    c->launches++;
+    CK(cudaMemcpyAsync(data, d_data, db, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
 extern "C" int ifos_fd_coeffs(const ifos_params *p, float *hc7) {
     if (!p || !hc7) return IFOS_ERR_ARG;
     return fd_coefficients(p->fdorder, p->maxrelerror, hc7) ? IFOS_OK : IFOS_ERR_ARG;

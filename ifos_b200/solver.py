@@ -225,6 +225,15 @@ class ShotSolver:
                                                    en.ctypes.data_as(DP)))
         return l2, en
 
+    def timedomain_filt(self, data, fc, order, method=1, f_high_pass=0.0):
+        """Butterworth lowpass (method 1, then a highpass at f_high_pass when
+        non-zero) or highpass (method 2) of the traces of `data` (ntr, ns)
+        at the context's DT (src/timedomain_filt.c).  Returns a new array."""
+        d = _f32(data).copy()
+        self._check(self.lib.ifos_timedomain_filt(self._ctx, _fp(d), d.shape[0], d.shape[1], float(fc), int(order),
+                                                  int(method), float(f_high_pass)))
+        return d
+
     def trkill_table(self, rec_xy, src_xy, lower, upper, table=None):
         """Offset-based trace-kill table (src/create_trkill_table.c): rec_xy
         (2, ntr) receiver grid indices, src_xy (2, nsrc) source coordinates in

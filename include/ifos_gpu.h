@@ -263,6 +263,16 @@ enum {
 int ifos_set_option(ifos_ctx *ctx, int option, int value);
 int ifos_get_option(const ifos_ctx *ctx, int option, int *value);
 
+/* Butterworth filtering of ntr traces of ns samples (host, in place), as
+ * src/timedomain_filt.c does with the vendored libcseife: method 1 a lowpass
+ * of `order` at corner frequency fc, followed by a highpass at f_high_pass
+ * when that is non-zero (F_HIGH_PASS); method 2 a highpass at fc.  Each
+ * trace is filtered in double with a zero sample before it, as the
+ * reference's dvector provides; the context's DT is the sample interval.
+ * Orders up to 16. */
+int ifos_timedomain_filt(ifos_ctx *ctx, float *data, int ntr, int ns, float fc, int order, int method,
+                         float f_high_pass);
+
 /* Step length of the line search (src/calc_opt_step.c:73-112, solving with
  * src/solvelin.c:53-70): fits the parabola a + b*eps + c*eps^2 through the
  * misfits l2t[0..2] of the test steps epst[0..2] by Gaussian elimination
