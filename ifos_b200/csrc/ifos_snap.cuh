@@ -599,4 +599,39 @@ __global__ void k_butterworth(float *data, double *work, int ntr, int ns, KIIR l
     }
 }
 
+// Per-shot gradient taper around the source (src/taper_grad_shot.c:52-197,
+// sws=1): the taper matrix (gp x gp values, formed on the host as the
+// reference forms it) is centred on the source cell, every cell outside it
+// has the value 1, the field is shifted by its minimum and divided by its
+// maximum, the gradient is multiplied by it, and the cells within `filtsize`
+// of the source are set to zero.
+struct KTaperShot {
+    int i0, j0, ijc, gp;  // source cell, centre index of the taper matrix, its size
+    float minm, maxm;     // minimum of the tapered field and maximum after the shift
+    int filtsize;
+};
+__global__ void k_taper_shot(float *gout, long long n, int nx, int ny, unsigned planes, const KTaperShot *tp,
+                             const float *mats) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int slot = blockIdx.y;
+    if (q >= n) return;
+    const KTaperShot t = tp[slot];
+    const int i = (int)(q % nx) + 1, j = (int)(q / nx) + 1;
+    float msum = 1.0f;
+    const int ix = i - t.i0 + t.ijc, iy = j - t.j0 + t.ijc;
+    if (ix >= 1 && ix <= t.gp && iy >= 1 && iy <= t.gp) {
+        const float m = mats[(long long)slot * t.gp * t.gp + (long long)(iy - 1) * t.gp + (ix - 1)];
+        if (msum > m) msum = m;
+    }
+    const float coeff = (msum - t.minm) / t.maxm;
+    const bool zero = i >= t.i0 - t.filtsize && i <= t.i0 + t.filtsize && j >= t.j0 - t.filtsize &&
+                      j <= t.j0 + t.filtsize;
+    float *g = gout + (long long)slot * 10 * n + q;
+    for (int k = 0; k < 10; k++) {
+        if (!(planes >> k & 1u)) continue;
+        g[k * n] = zero ? 0.0f : g[k * n] * coeff;
+    }
+    (void)ny;
+}
+
 }  // namespace ifos

@@ -1722,6 +1722,100 @@ extern "C" int ifos_opt_step(const float *l2t, const float *epst, int fp64, floa
     return IFOS_OK;
 }
 
+// The taper matrix of src/taper_grad_shot.c:62-111 (gp x gp floats, row j
+// then column i), with the reference's float/double promotions.
+static std::vector<float> shot_taper_matrix(float srtradius, int srtshape, float dh, int &gp) {
+    gp = (int)(std::ceil(2.0 * srtradius / dh));
+    if (gp < 5) gp = 5;
+    std::vector<float> m((size_t)gp * gp);
+    const float a = 1.0f;
+    const float maxrad = (float)std::sqrt(2.0 * srtradius * srtradius);
+    for (int j = 1; j <= gp; j++)
+        for (int i = 1; i <= gp; i++) {
+            const float x = (float)(((float)i - ((float)gp) / 2.0 - 0.5) * dh);
+            const float y = (float)(((float)j - ((float)gp) / 2.0 - 0.5) * dh);
+            // the reference calls the double sqrt / erf / log on float arguments
+            const float rad = (float)std::sqrt((double)(x * x + y * y));
+            float v = 0.0f;
+            if (srtshape == 1) v = (float)std::erf((double)(a * rad / maxrad));
+            else if (rad > 0) v = (float)std::log((double)rad);
+            m[(size_t)(j - 1) * gp + (i - 1)] = v;
+        }
+    // minimum_m / maximum_m of src/util.c:56-90: start at [1][1], then compare
+    auto at = [&](int j, int i) -> float & { return m[(size_t)(j - 1) * gp + (i - 1)]; };
+    float minm = at(1, 1);
+    for (int i = 1; i <= gp; i++)
+        for (int j = 1; j <= gp; j++)
+            if (i * j != 1 && at(j, i) < minm) minm = at(j, i);
+    for (float &v : m) v -= minm;
+    const float edge[4] = {at(1, gp / 2), at(gp / 2, 1), at(gp / 2, gp), at(gp, gp / 2)};
+    float maxm = edge[0];
+    for (int k = 1; k < 4; k++)
+        if (edge[k] > maxm) maxm = edge[k];
+    for (float &v : m) {
+        v /= maxm;
+        if (v > 1.0f) v = 1.0f;
+    }
+    return m;
+}
+
+extern "C" int ifos_taper_grad_shot(ifos_ctx *c, int nshots, const float *src_xy, float srtradius, int srtshape,
+                                    int filtsize, unsigned planes) {
+    if (!c || !src_xy || nshots < 1 || nshots > c->p.max_shots) return IFOS_ERR_ARG;
+    if (srtshape != 1 && srtshape != 2) return fail(c, IFOS_ERR_ARG, "SRTSHAPE must be 1 or 2");
+    CK(cudaSetDevice(c->device));
+    const ifos_params &p = c->p;
+    const float dh = p.dh;
+    int gp = 0;
+    const std::vector<float> mat = shot_taper_matrix(srtradius, srtshape, dh, gp);
+    const int ijc = (int)std::ceil((float)gp / 2);
+    std::vector<KTaperShot> tp(nshots);
+    std::vector<float> mats((size_t)nshots * gp * gp);
+    for (int s = 0; s < nshots; s++) {
+        KTaperShot &t = tp[s];
+        t.i0 = (int)std::floor(src_xy[2 * s] / dh + 0.5);  // iround(srcpos[1][n]/DH)
+        t.j0 = (int)std::floor(src_xy[2 * s + 1] / dh + 0.5);
+        t.ijc = ijc;
+        t.gp = gp;
+        t.filtsize = filtsize;
+        std::copy(mat.begin(), mat.end(), mats.begin() + (size_t)s * gp * gp);
+        // the field's minimum over every cell (1 outside the taper, which is at most 1 inside)
+        bool outside = (long long)p.nx * p.ny > 0;
+        int inside = 0;
+        float minm = 1.0f;
+        for (int iy = 1; iy <= gp; iy++)
+            for (int ix = 1; ix <= gp; ix++) {
+                const int xx = t.i0 + ix - ijc, yy = t.j0 + iy - ijc;
+                if (xx < 1 || xx > p.nx || yy < 1 || yy > p.ny) continue;
+                inside++;
+                const float v = std::min(1.0f, mat[(size_t)(iy - 1) * gp + (ix - 1)]);
+                if (v < minm) minm = v;
+            }
+        outside = inside < p.nx * p.ny;
+        float maxm = outside ? 1.0f - minm : -INFINITY;
+        for (int iy = 1; iy <= gp; iy++)
+            for (int ix = 1; ix <= gp; ix++) {
+                const int xx = t.i0 + ix - ijc, yy = t.j0 + iy - ijc;
+                if (xx < 1 || xx > p.nx || yy < 1 || yy > p.ny) continue;
+                const float v = std::min(1.0f, mat[(size_t)(iy - 1) * gp + (ix - 1)]) - minm;
+                if (v > maxm) maxm = v;
+            }
+        t.minm = minm;
+        t.maxm = maxm;
+    }
+    const size_t tb = ((size_t)nshots * sizeof(KTaperShot) + 255) / 256 * 256;
+    void *scr = nullptr;
+    if (int rc = scratch(c, tb + mats.size() * 4, &scr)) return rc;
+    CK(cudaMemcpyAsync(scr, tp.data(), nshots * sizeof(KTaperShot), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((char *)scr + tb, mats.data(), mats.size() * 4, cudaMemcpyHostToDevice, c->st));
+    const long long N = (long long)p.nx * p.ny;
+    k_taper_shot<<<dim3((unsigned)((N + 255) / 256), (unsigned)nshots), 256, 0, c->st>>>(
+        (float *)c->gout.p, N, p.nx, p.ny, planes, (const KTaperShot *)scr, (const float *)((char *)scr + tb));
+    c->launches++;
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
 // The cascade of a Butterworth filter of order `m` (contrib/libcseife/
 // cseife.c:164-193 with the section coefficients of cseife_rfk.c): a first-
 // order section when m is odd, then m/2 second-order sections with damping

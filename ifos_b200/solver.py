@@ -225,6 +225,19 @@ class ShotSolver:
                                                    en.ctypes.data_as(DP)))
         return l2, en
 
+    def taper_grad_shot(self, src_xy, nshots=1, srtradius=5.0, srtshape=1, filtsize=1,
+                        planes=(3, 4, 5, 8, 9)):
+        """Taper the stored per-shot gradients of slots [0, nshots) around
+        each source (src/taper_grad_shot.c, sws=1); src_xy (nshots, 2) in
+        metres; planes: IFOS_G_* indices (default the assembled vp, vs, rho
+        and SH vs, rho gradients).  Fetch them with ``fetch_grads``."""
+        xy = np.ascontiguousarray(src_xy, np.float32).reshape(nshots, 2)
+        mask = 0
+        for k in planes:
+            mask |= 1 << int(k)
+        self._check(self.lib.ifos_taper_grad_shot(self._ctx, int(nshots), _fp(xy), float(srtradius), int(srtshape),
+                                                  int(filtsize), mask))
+
     def timedomain_filt(self, data, fc, order, method=1, f_high_pass=0.0):
         """Butterworth lowpass (method 1, then a highpass at f_high_pass when
         non-zero) or highpass (method 2) of the traces of `data` (ntr, ns)

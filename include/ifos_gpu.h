@@ -273,6 +273,15 @@ int ifos_get_option(const ifos_ctx *ctx, int option, int *value);
 int ifos_timedomain_filt(ifos_ctx *ctx, float *data, int ntr, int ns, float fc, int order, int method,
                          float f_high_pass);
 
+/* Per-shot gradient taper around the source (src/taper_grad_shot.c, sws=1)
+ * applied on the device to the stored per-shot gradients of slots
+ * [0, nshots) (the planes of `planes`, a bit mask over IFOS_G_*), as the
+ * driver applies it before summing the shots (src/IFOS2D.c:2683-2687):
+ * src_xy holds each slot's source x, y in metres (srcpos rows 1-2);
+ * srtradius, srtshape and filtsize are SRTRADIUS, SRTSHAPE and FILTSIZE. */
+int ifos_taper_grad_shot(ifos_ctx *ctx, int nshots, const float *src_xy, float srtradius, int srtshape,
+                         int filtsize, unsigned planes);
+
 /* Step length of the line search (src/calc_opt_step.c:73-112, solving with
  * src/solvelin.c:53-70): fits the parabola a + b*eps + c*eps^2 through the
  * misfits l2t[0..2] of the test steps epst[0..2] by Gaussian elimination

@@ -47,3 +47,45 @@ def test_butterworth_matches_timedomain_filt(fc, order, method, fhp):
         got = s.timedomain_filt(data, fc, order, method, fhp)
     assert np.array_equal(got.view(np.int32), want.view(np.int32))
     assert not np.array_equal(got, data)
+
+
+@pytest.mark.parametrize("srtradius,srtshape,filtsize,sx", [(5.0, 1, 1, 20.3), (3.0, 2, 2, 3.0), (12.0, 1, 0, 61.0)])
+def test_shot_taper_matches_taper_grad_shot(srtradius, srtshape, filtsize, sx):
+    """The per-shot source taper on the device-resident gradients against
+    src/taper_grad_shot.c (sws=1) on the same per-shot gradient planes."""
+    from ifos_b200.solver import ShotSolver
+    from tests.golden.cases import build_case
+    p, model, g, sig, adj = build_case("psv_el_o4")
+    ref, _ = H.libs()
+    sy = 3.0 * p.dh
+    with ShotSolver(p, max_rec=g.recpos.shape[1]) as s:
+        s.upload_model(model)
+        s.setup_shot(0, g.srcpos, sig, g.recpos)
+        s.forward(1, store=True, fetch=False)
+        before = s.adjoint(adj[None])[0]
+        s.taper_grad_shot([[sx, sy]], 1, srtradius, srtshape, filtsize, planes=(3, 4, 5))
+        after = s.fetch_grads(1)[0]
+    for name, v in (("NX", p.nx), ("NY", p.ny), ("NXG", p.nx), ("NYG", p.ny), ("FREE_SURF", 1), ("NPROCX", 1),
+                    ("NPROCY", 1), ("MYID", 0), ("VERBOSE", 0), ("SRTSHAPE", srtshape), ("FILTSIZE", filtsize)):
+        C.c_int.in_dll(ref, name).value = v
+    C.c_float.in_dll(ref, "DH").value = p.dh
+    C.c_float.in_dll(ref, "SRTRADIUS").value = srtradius
+    pos = (C.c_int * 3).in_dll(ref, "POS")
+    pos[0] = pos[1] = pos[2] = 0
+    T = ref.matrix(1, p.ny, 1, p.nx)
+    SP = ref.matrix(1, 8, 1, 1)
+    SP[1][1], SP[2][1] = sx, sy
+    R = ref.imatrix(1, 3, 1, 1)
+    f = ref.taper_grad_shot
+    f.restype = None
+    f.argtypes = [H.FPP, H.FPP, H.FPP, C.c_int, H.IPP, C.c_int, C.c_int, C.c_int]
+    for k in (3, 4, 5):
+        W_ = ref.matrix(1, p.ny, 1, p.nx)
+        for j in range(p.ny):
+            for i in range(p.nx):
+                W_[j + 1][i + 1] = float(before[k, j, i])
+        f(W_, T, SP, 1, R, 1, 1, 1)
+        want = np.array([[W_[j + 1][i + 1] for i in range(p.nx)] for j in range(p.ny)], np.float32)
+        assert np.array_equal(after[k].view(np.int32), want.view(np.int32)), k
+        assert not np.array_equal(after[k], before[k])
+    assert np.array_equal(after[[0, 1, 2, 6, 7]], before[[0, 1, 2, 6, 7]])  # planes not asked for are untouched
