@@ -634,4 +634,61 @@ __global__ void k_taper_shot(float *gout, long long n, int nx, int ny, unsigned 
     (void)ny;
 }
 
+// Median smoothing of a gradient or model plane (src/smooth.c with
+// src/median2D.c).  Every cell takes the window of fs x fs values around it
+// (edges extended by the nearest row / column), gathered x-major as the
+// reference's filterpart is.  The reference sorts its vector t[0..k-1] with
+// t[0] = 0 (a zeroed element before the copied window) and t[1..k-1] the
+// first k-1 window values, leaving the last window value at t[k], and returns
+// t[k/2+1]; the same non-recursive quicksort (src/util.c:437-466) runs here
+// so that ties of +0 and -0 resolve as they do there.
+constexpr int kMedianMax = 31 * 31 + 1;
+__device__ __forceinline__ void quicksort_dev(float *arr, int elements) {
+    int beg[64], end[64], i = 0;
+    beg[0] = 0;
+    end[0] = elements;
+    while (i >= 0) {
+        int L = beg[i], R = end[i] - 1;
+        if (L < R) {
+            const float piv = arr[L];
+            while (L < R) {
+                while (arr[R] >= piv && L < R) R--;
+                if (L < R) arr[L++] = arr[R];
+                while (arr[L] <= piv && L < R) L++;
+                if (L < R) arr[R--] = arr[L];
+            }
+            arr[L] = piv;
+            beg[i + 1] = L + 1;
+            end[i + 1] = end[i];
+            end[i++] = L;
+            if (end[i] - beg[i] > end[i - 1] - beg[i - 1]) {
+                int sw = beg[i];
+                beg[i] = beg[i - 1];
+                beg[i - 1] = sw;
+                sw = end[i];
+                end[i] = end[i - 1];
+                end[i - 1] = sw;
+            }
+        } else {
+            i--;
+        }
+    }
+}
+__global__ void k_median_smooth(const float *in, float *out, int nx, int ny, int fs) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= (long long)nx * ny) return;
+    const int i = (int)(q % nx) + 1, j = (int)(q / nx) + 1;
+    const int hfs = fs / 2, k = fs * fs;
+    float t[kMedianMax];
+    t[0] = 0.0f;
+    int n = 1;
+    for (int ii = -hfs; ii <= hfs; ii++)
+        for (int jj = -hfs; jj <= hfs; jj++) {
+            const int x = min(max(i + ii, 1), nx), y = min(max(j + jj, 1), ny);
+            t[n++] = in[(long long)(y - 1) * nx + (x - 1)];
+        }
+    quicksort_dev(t, k);
+    out[q] = t[k / 2 + 1];
+}
+
 }  // namespace ifos

@@ -1816,6 +1816,26 @@ extern "C" int ifos_taper_grad_shot(ifos_ctx *c, int nshots, const float *src_xy
     return IFOS_OK;
 }
 
+extern "C" int ifos_median_smooth(ifos_ctx *c, float *mat, int filt_size) {
+    if (!c || !mat) return IFOS_ERR_ARG;
+    if (filt_size == 0) return IFOS_OK;  // src/smooth.c:78 returns unchanged
+    int fs = filt_size;
+    if (!(fs % 2)) fs += fs > 0 ? 1 : -1;  // an even size grows away from zero (src/smooth.c:79-82)
+    fs = std::abs(fs);
+    if (fs * fs + 1 > kMedianMax) return fail(c, IFOS_ERR_ARG, "filter size above 31");
+    CK(cudaSetDevice(c->device));
+    const long long N = (long long)c->p.nx * c->p.ny;
+    void *scr = nullptr;
+    if (int rc = scratch(c, (size_t)2 * N * 4, &scr)) return rc;
+    float *d_in = (float *)scr, *d_out = d_in + N;
+    CK(cudaMemcpyAsync(d_in, mat, (size_t)N * 4, cudaMemcpyHostToDevice, c->st));
+    k_median_smooth<<<(unsigned)((N + 127) / 128), 128, 0, c->st>>>(d_in, d_out, c->p.nx, c->p.ny, fs);
+    c->launches++;
+    CK(cudaMemcpyAsync(mat, d_out, (size_t)N * 4, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
 // The cascade of a Butterworth filter of order `m` (contrib/libcseife/
 // cseife.c:164-193 with the section coefficients of cseife_rfk.c): a first-
 // order section when m is odd, then m/2 second-order sections with damping

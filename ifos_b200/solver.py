@@ -238,6 +238,13 @@ class ShotSolver:
         self._check(self.lib.ifos_taper_grad_shot(self._ctx, int(nshots), _fp(xy), float(srtradius), int(srtshape),
                                                   int(filtsize), mask))
 
+    def median_smooth(self, plane, filt_size):
+        """Median smoothing of an NY x NX plane (src/smooth.c); returns a
+        new array."""
+        m = _f32(plane).copy()
+        self._check(self.lib.ifos_median_smooth(self._ctx, _fp(m), int(filt_size)))
+        return m
+
     def timedomain_filt(self, data, fc, order, method=1, f_high_pass=0.0):
         """Butterworth lowpass (method 1, then a highpass at f_high_pass when
         non-zero) or highpass (method 2) of the traces of `data` (ntr, ns)

@@ -282,6 +282,12 @@ int ifos_timedomain_filt(ifos_ctx *ctx, float *data, int ntr, int ns, float fc, 
 int ifos_taper_grad_shot(ifos_ctx *ctx, int nshots, const float *src_xy, float srtradius, int srtshape,
                          int filtsize, unsigned planes);
 
+/* Median smoothing of an NY x NX plane (host, in place) as src/smooth.c
+ * does for gradients (FILT_SIZE_GRAD) and models (FILT_SIZE): filt_size 0
+ * leaves the plane unchanged, an even size grows away from zero, |size| up
+ * to 31; bit-identical to the reference's median2d selection. */
+int ifos_median_smooth(ifos_ctx *ctx, float *mat, int filt_size);
+
 /* Step length of the line search (src/calc_opt_step.c:73-112, solving with
  * src/solvelin.c:53-70): fits the parabola a + b*eps + c*eps^2 through the
  * misfits l2t[0..2] of the test steps epst[0..2] by Gaussian elimination

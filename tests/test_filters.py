@@ -89,3 +89,36 @@ def test_shot_taper_matches_taper_grad_shot(srtradius, srtshape, filtsize, sx):
         assert np.array_equal(after[k].view(np.int32), want.view(np.int32)), k
         assert not np.array_equal(after[k], before[k])
     assert np.array_equal(after[[0, 1, 2, 6, 7]], before[[0, 1, 2, 6, 7]])  # planes not asked for are untouched
+
+
+@pytest.mark.parametrize("filt_size", [3, 4, 7, -5])
+def test_median_smoothing_matches_smooth(filt_size):
+    """Median smoothing of a plane against src/smooth.c (filter 2, FILT_SIZE)
+    with src/median2D.c, including its window selection and the +0/-0 ties
+    of its quicksort (the plane holds both zeros)."""
+    from ifos_b200.params import ShotParams
+    from ifos_b200.solver import ShotSolver
+    rng = np.random.default_rng(abs(filt_size))
+    ny, nx = 23, 37
+    plane = rng.standard_normal((ny, nx)).astype(np.float32)
+    plane[rng.uniform(size=plane.shape) < 0.15] = 0.0
+    plane[rng.uniform(size=plane.shape) < 0.15] = -0.0
+    ref, _ = H.libs()
+    for name, v in (("NX", nx), ("NY", ny), ("NXG", nx), ("NYG", ny), ("NPROCX", 1), ("NPROCY", 1), ("MYID", 0),
+                    ("VERBOSE", 0), ("FILT_SIZE", filt_size)):
+        C.c_int.in_dll(ref, name).value = v
+    pos = (C.c_int * 3).in_dll(ref, "POS")
+    pos[0] = pos[1] = pos[2] = 0
+    M = ref.matrix(1, ny, 1, nx)
+    for j in range(ny):
+        for i in range(nx):
+            M[j + 1][i + 1] = float(plane[j, i])
+    f = ref.smooth
+    f.restype = None
+    f.argtypes = [H.FPP, C.c_int, C.c_int, C.c_float, C.c_float]
+    f(M, 1, 2, 0.0, 0.0)
+    want = np.array([[M[j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
+    p = ShotParams(nx=nx, ny=ny, nt=20, dh=1.0, dt=1e-3, fdorder=4, fw=4)
+    with ShotSolver(p, snapshots=False) as s:
+        got = s.median_smooth(plane, filt_size)
+    assert np.array_equal(got.view(np.int32), want.view(np.int32))
