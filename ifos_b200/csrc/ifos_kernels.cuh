@@ -653,20 +653,25 @@ __device__ __forceinline__ bool psource_fires(const KSrc &src, int slot) {
     const float *pos = src.pos + (long long)slot * 8 * src.max_src;
     return (int)pos[7 * src.max_src + n - 1] == 1;
 }
-// source l of a slot at its cell
-template <typename T>
-__device__ void psource_apply(const KGrid &g, const KState<T> &S, const KSrc &src, int nt, int acoustic,
-                              const KSnapPatch &pt, int slot, int l) {
-    const float *pos = src.pos + (long long)slot * 8 * src.max_src;
+// the explosive source term of source l at step nt (src/psource.c:47-52):
+// the centred difference of its signal over 2 DH^2, one-sided at the ends
+__device__ __forceinline__ float psource_amp(const KSrc &src, int slot, int l, int nt, float DH) {
     const float *sig = src.sig + (long long)slot * src.max_src * src.nt_total;
     const int NT = src.nt_total;
-    const float DH = g.dh;
-    const int i = (int)pos[l], j = (int)pos[src.max_src + l];
     const float *sl = sig + (long long)l * NT - 1;
     float amp = 0.0f;
     if (nt == 1) amp = sl[nt + 1] / (2.0 * DH * DH);
     if ((nt > 1) && (nt < NT)) amp = (sl[nt + 1] - sl[nt - 1]) / (2.0 * DH * DH);
     if (nt == NT) amp = -sl[nt - 1] / (2.0 * DH * DH);
+    return amp;
+}
+// source l of a slot at its cell
+template <typename T>
+__device__ void psource_apply(const KGrid &g, const KState<T> &S, const KSrc &src, int nt, int acoustic,
+                              const KSnapPatch &pt, int slot, int l) {
+    const float *pos = src.pos + (long long)slot * 8 * src.max_src;
+    const int i = (int)pos[l], j = (int)pos[src.max_src + l];
+    const float amp = psource_amp(src, slot, l, nt, g.dh);
     const long long c = pidx(g, j, i);
     if (!acoustic) {
         T *sxx = fieldp(S, slot, P_SXX), *syy = fieldp(S, slot, P_SYY);

@@ -863,6 +863,10 @@ struct Launcher {
     KRec rec;
     dim3 blk{32, 8, 1}, grd;
     int nshots;
+    // the stress ops apply the explosive sources (fps) and the free surface
+    // (fsurf) of step nt_cur themselves: P-SV elastic and viscoelastic only
+    int nt_cur = 0, fsurf = 0, fps = 0;
+    int src_j0 = 1, src_j1 = 0;  // rows holding the slots' sources (empty range: none)
     Launcher(ifos_ctx *cc, int ns) : c(cc), nshots(ns) {
         S = kstate<T>(c);
         M = kmodel<T>(c);
@@ -946,11 +950,14 @@ struct Launcher {
             bool done = false;
             if constexpr (FD >= 5) {
                 if (g.quirk_hi) {
-                    pipelined(OpSVisc<FD, kTileY, LL, NST, true>{g, S, M, c->ktma, snap_out(hin)});
+                    pipelined(OpSVisc<FD, kTileY, LL, NST, true>{g, S, M, c->ktma, snap_out(hin), src, nt_cur, fsurf,
+                                                                 fps, src_j0, src_j1});
                     done = true;
                 }
             }
-            if (!done) pipelined(OpSVisc<FD, kTileY, LL, NST, false>{g, S, M, c->ktma, snap_out(hin)});
+            if (!done)
+                pipelined(OpSVisc<FD, kTileY, LL, NST, false>{g, S, M, c->ktma, snap_out(hin), src, nt_cur, fsurf, fps, src_j0,
+                                                              src_j1});
         }
         if (c->sh) pipelined(OpSSh<FD, kTileY, LL, ring_stages<FD, 1, 2 + 2 * LL + 4, 0>()>{g, S, M, c->ktma, snap_out(hin)});
     }
@@ -978,11 +985,11 @@ struct Launcher {
                     bool done = false;
                     if constexpr (FD >= 5) {
                         if (quirk) {
-                            pipelined(OpSEl<FD, kTileY, NST, true>{g, S, M, t, snap_out(hin)});
+                            pipelined(OpSEl<FD, kTileY, NST, true>{g, S, M, t, snap_out(hin), src, nt_cur, fsurf, fps, src_j0, src_j1});
                             done = true;
                         }
                     }
-                    if (!done) pipelined(OpSEl<FD, kTileY, NST, false>{g, S, M, t, snap_out(hin)});
+                    if (!done) pipelined(OpSEl<FD, kTileY, NST, false>{g, S, M, t, snap_out(hin), src, nt_cur, fsurf, fps, src_j0, src_j1});
                 }
                 if (c->sh) pipelined(OpSSh<FD, kTileY, 0, ring_stages<FD, 1, 4, 0>()>{g, S, M, t, snap_out(hin)});
                 break;
@@ -1035,7 +1042,7 @@ struct Launcher {
     // the explosive sources, free surface and receivers of a forward step
     void post_fwd(int nt, bool psource, const KSnapPatch &pt) {
         const KGrid &g = c->g;
-        if (psource || c->p.free_surf) {
+        if (!fps && (psource || c->p.free_surf)) {
             const dim3 gs((unsigned)((c->p.nx + 127) / 128), (unsigned)nshots);
             DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_surface_src<T, FD>, gs, dim3(128), 0, g, S, M, src, nt,
                                              c->psv, c->sh, c->ac, psource ? 1 : 0, c->p.free_surf ? 1 : 0, pt));
@@ -1054,7 +1061,7 @@ struct Launcher {
             launch_dep(c->st, c->pdl, k_psource_adj<T>, gr, dim3(128), 0, g, S, rec, nt, c->ac);
             c->launches++;
         }
-        if (c->p.free_surf) {
+        if (c->p.free_surf && !fsurf) {
             const dim3 gs((unsigned)((c->p.nx + 127) / 128), (unsigned)nshots);
             DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_surface_src<T, FD>, gs, dim3(128), 0, g, S, M, src, nt,
                                              c->psv, c->sh, c->ac, 0, 1, KSnapPatch{}));
@@ -1167,6 +1174,24 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     // holding them are stored again after it
     const bool fused = snaps && c->pipe && c->fused_snap;
     const bool f16s = p.snap_format == IFOS_SNAP_F16S;
+    // P-SV elastic / viscoelastic: the stress kernel applies the explosive
+    // sources and the free surface, so nothing changes a stress after it
+    // (no surface kernel, no snapshot patches)
+    const bool in_stress = c->pipe && c->psv && !c->ac && !c->sh;
+    Lr.fps = in_stress ? 1 : 0;
+    Lr.fsurf = (in_stress && p.free_surf) ? 1 : 0;
+    {
+        const int ms = std::max(1, p.max_src);
+        int lo = p.ny + 1, hi = 0;
+        for (int s = 0; s < nshots; s++)
+            for (int l = 0; l < c->nsrc_h[s]; l++) {
+                const int j = (int)c->srcpos_h[(size_t)s * 8 * ms + ms + l];
+                lo = std::min(lo, j);
+                hi = std::max(hi, j);
+            }
+        Lr.src_j0 = lo;
+        Lr.src_j1 = hi;
+    }
     const int segs = (p.nx + 63) / 64;
     KSnapPatch pt{};
     pt.slot_floats = c->snap_slot_bytes / 4;
@@ -1187,7 +1212,9 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         const bool snap_now = snaps && ((nt - 1) % p.dtinv == 0) && hin < ntd;
         const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
         const int fhin = (fused && snap_now) ? hin : -1;
-        pt.base = (fhin >= 0 && !f16s) ? (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes) : nullptr;
+        pt.base = (fhin >= 0 && !f16s && !in_stress) ? (float *)((char *)c->snap.p + (size_t)hin * c->snap_bytes)
+                                                     : nullptr;
+        Lr.nt_cur = nt;
         {
             KTimer t(c, 0, sample);
             Lr.v_step(0, snap_now ? 1 : 0, fhin);
@@ -1203,7 +1230,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         }
         Lr.post_fwd(nt, c->psv != 0, pt);
         if (snap_now && fused) {
-            if (f16s && (p.free_surf || c->psv)) {
+            if (f16s && !in_stress && (p.free_surf || c->psv)) {
                 const int4 patched = make_int4(pt.c_sxx, pt.c_syy, pt.c_sp, pt.c_syz);
                 launch_dep(c->st, c->pdl, k_snap_fix16<T>, dim3(segs + std::max(1, p.max_src), 1, nshots), dim3(32),
                            0, c->g, Lr.S, sn, hin, Lr.src, p.free_surf ? 1 : 0, patched);
@@ -1228,7 +1255,10 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         }
     }
     };
-    if (int rc = run_loop(c, c->gfwd, loop_key(c, {0, nshots, snaps, nsteps, force, fused}), enqueue)) return rc;
+    // the source rows are launch parameters of the stress kernels: part of the captured sequence
+    if (int rc = run_loop(c, c->gfwd, loop_key(c, {0, nshots, snaps, nsteps, force, fused, Lr.src_j0, Lr.src_j1}),
+                          enqueue))
+        return rc;
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));
@@ -1247,6 +1277,9 @@ template <typename T>
 static int adjoint_t(ifos_ctx *c, int nshots) {
     const ifos_params &p = c->p;
     Launcher<T> Lr(c, nshots);
+    // P-SV elastic / viscoelastic without the pressure residual source: the
+    // stress kernel applies the free surface (no surface kernel)
+    Lr.fsurf = (c->pipe && c->psv && !c->ac && !c->sh && p.free_surf && p.adjoint_type != 4) ? 1 : 0;
     if (int rc = zero_state<T>(c, nshots)) return rc;
     const long long N = (long long)p.nx * p.ny;
     CK(cudaMemsetAsync(c->gacc.p, 0, (size_t)nshots * 5 * N * 4, c->st));

@@ -452,22 +452,107 @@ __device__ __forceinline__ void release_stage(uint64_t *empty) {
     if (threadIdx.x == 0) mbar_arrive(empty);
 }
 
+// Explosive sources of step nt on row j, as src/psource.c:47-55 applies
+// them after the stress update and before the free surface
+// (src/IFOS2D.c:1758-1764): the lane holding a source cell adds half the
+// source term to its sxx and syy, sources in list order (psource_apply).
+__device__ __forceinline__ void psource_row(const KGrid &g, const KSrc &src, int slot, int nt, int j, const Cols &cl,
+                                            float (&sxx)[2], float (&syy)[2]) {
+    if (!psource_fires(src, slot)) return;
+    const int n = src.nsrc[slot];
+    const float *pos = src.pos + (long long)slot * 8 * src.max_src;
+    for (int l = 0; l < n; l++) {
+        if ((int)pos[src.max_src + l] != j) continue;
+        const int e = (int)pos[l] - cl.i;
+        if ((e != 0 && e != 1) || !cl.valid(e)) continue;
+        const float amp = psource_amp(src, slot, l, nt, g.dh);
+        if (e == 0) {
+            sxx[0] = (float)((double)sxx[0] + 0.5 * (double)amp);
+            syy[0] = (float)((double)syy[0] + 0.5 * (double)amp);
+        } else {
+            sxx[1] = (float)((double)sxx[1] + 0.5 * (double)amp);
+            syy[1] = (float)((double)syy[1] + 0.5 * (double)amp);
+        }
+    }
+}
+
+// The free surface of row 1 on a stress op's results (surface_cell: the
+// elastic src/surface_elastic_PML.c:53-104 and, with L memory variables, the
+// viscoelastic src/surface_PML.c:60-157), from the staged velocities (wx:
+// the vx window of row 1; vy2: the zero-started y difference of vy, formed
+// before the stage was released): the derivatives are zero-started sums
+// scaled by 1/DH, vxx carries its own x CPML (psi_vxxs).  p and q are the
+// p and q memory variables (LL each).
+template <int FDOH, int HE, int LL>
+__device__ __forceinline__ void surface_row(const KGrid &g, const KState<float> &S, const KModel<float> &M,
+                                            const Hc<FDOH> &hc, const XWin<HE> &wx, float2 vy2, const Cols &cl,
+                                            int slot, int model, float (&sxx)[2], float (&syy)[2], float (*p)[2],
+                                            float (*q)[2]) {
+    const float DT = g.dt, DH = g.dh;
+    const float dh24 = (float)(1.0 / (double)DH), dthalbe = (float)((double)DT / 2.0);
+    const float *srf = M.srf + (long long)model * M.srf_stride;
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+        if (!cl.valid(e)) continue;
+        const int i = cl.i + e;
+        syy[e] = 0.0f;
+#pragma unroll
+        for (int l = 0; l < LL; l++) q[l][e] = 0.0f;
+        float vxx = xbwd<FDOH, HE, true>(hc, wx, e) * dh24;
+        const float vyy = pick(vy2, e) * dh24;
+        const int hx = strip_x(g, i);  // the surface has its x CPML also where the stress update has none (10/12)
+        if (hx) vxx = pml_x(g, M, S.psix[X_VXXS] + slot * S.psix_slot, 1, hx, K_X, A_X, B_X, vxx);
+        const float fjm = srf[i - 1], gg = srf[g.nx + i - 1];
+        if (LL == 0) {
+            sxx[e] += -DT * ((gg * gg) / (gg + fjm) * vxx + gg * vyy);
+            continue;
+        }
+        const float djm = srf[2 * g.nx + i - 1], ee = srf[3 * g.nx + i - 1];
+        float sump = 0;
+#pragma unroll
+        for (int l = 0; l < LL; l++) sump += p[l][e];
+        sxx[e] += -(DT * (gg - fjm) * (gg - fjm) * vxx / gg) - (DT * (gg - fjm) * vyy) - (dthalbe * sump);
+        sump = 0;
+#pragma unroll
+        for (int l = 0; l < LL; l++) {
+            const float bjm = g.bjm_srf[l + 1];
+            p[l][e] = (float)((double)p[l][e] + (double)bjm * (((double)(djm - ee) * ((double)(fjm / gg) - 1.0) *
+                                                                 (double)vxx) - (double)((djm - ee) * vyy)));
+            sump += p[l][e];
+        }
+        sxx[e] += (dthalbe * sump);
+    }
+}
+
 // Interior tiles take rows<false>; tiles with a strip cell rows<true>.
+// The path is chosen per warp (all lanes take the same one, so that the
+// warp-wide operations of the snapshot store and the stage release meet):
+// lanes outside the strips of a strip tile see hx = 0 and no y strip.
 #define IFOS_TILE_COMPUTE(NOPML_)                                                                     \
     __device__ __forceinline__ void compute(const TileInfo &ti, const float *h, const float *pl,      \
                                             uint64_t *empty) const {                                  \
         const Cols cl(g, ti, P::XH, !(NOPML_));                                                       \
-        if ((NOPML_) || (cl.hx0 == 0 && cl.hx1 == 0 && !ti.ystrip)) rows<false>(ti, cl, h, pl, empty); \
-        else rows<true>(ti, cl, h, pl, empty);                                                        \
+        if ((NOPML_) || (!__any_sync(0xffffffffu, cl.hx0 != 0 || cl.hx1 != 0) && !ti.ystrip))         \
+            rows<false>(ti, cl, h, pl, empty);                                                        \
+        else                                                                                          \
+            rows<true>(ti, cl, h, pl, empty);                                                         \
     }
 
 // the common members of an op
+// src, nt, fsurf, fps: the stress ops apply the explosive sources of step nt
+// (fps; rows src_j0..src_j1 hold every slot's sources) and the free surface
+// of row 1 (fsurf) themselves
 #define IFOS_OP_MEMBERS \
     KGrid g;            \
     KState<float> S;    \
     KModel<float> M;    \
     KTma tm;            \
-    KSnapOut so;
+    KSnapOut so;        \
+    KSrc src;           \
+    int nt;             \
+    int fsurf;          \
+    int fps;            \
+    int src_j0, src_j1;
 
 // ---------------------------------------------------------------------------
 // stress, P-SV viscoelastic with LL SLS (src/update_s_visc_PML.c; the
@@ -506,6 +591,7 @@ struct OpSVisc {
                                          uint64_t *empty) const {
         constexpr int RT = P::RT;
         const float *t_vx = h, *t_vy = h + P::BOXS;
+        float2 vys = make_float2(0.0f, 0.0f);  // the free surface's vy difference (row 1)
         const Hc<FDOH> hc(g);
         // everything this warp needs from the stage, then release it
         XWin<P::HE> wx[RT], wy[RT];
@@ -517,6 +603,7 @@ struct OpSVisc {
             wy[r].load(t_vy + (jj + P::H) * P::BW, cl.c0);
             dxy[r] = yfwd2<false, false, P, FDOH, QUIRK>(hc, t_vx, jj, cl.c0);
             dyy[r] = ybwd2<false, false, P, FDOH, QUIRK>(hc, t_vy, jj, cl.c0);
+            if (fsurf && ti.j0 + jj == 1) vys = ybwd2<false, false, P, FDOH, true>(hc, t_vy, jj, cl.c0);
 #pragma unroll
             for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
         }
@@ -598,6 +685,10 @@ struct OpSVisc {
                 o[1][e] = s_yy + (dthalbe * sumq);
                 o[2][e] = s_xy + (dthalbe * sumr);
             }
+            if (fps && j >= src_j0 && j <= src_j1) psource_row(g, src, slot, nt, j, cl, o[0], o[1]);
+            if (fsurf && j == 1)
+                surface_row<FDOH, P::HE, LL>(g, S, M, hc, wx[r], vys, cl, slot, ti.model, o[0], o[1], &o[3 + LL],
+                                             &o[3 + 2 * LL]);
             const RowOut out(g, S, so, slot, j, cl);
             out.put(S.off[P_SXX], o[0][0], o[0][1]);
             out.put(S.off[P_SYY], o[1][0], o[1][1]);
@@ -641,6 +732,7 @@ struct OpSEl {
                                          uint64_t *empty) const {
         constexpr int RT = P::RT;
         const float *t_vx = h, *t_vy = h + P::BOXS;
+        float2 vys = make_float2(0.0f, 0.0f);  // the free surface's vy difference (row 1)
         const Hc<FDOH> hc(g);
         XWin<P::HE> wx[RT], wy[RT];
         float2 dxy[RT], dyy[RT], in[RT][NP_];
@@ -651,6 +743,7 @@ struct OpSEl {
             wy[r].load(t_vy + (jj + P::H) * P::BW, cl.c0);
             dxy[r] = yfwd2<false, false, P, FDOH>(hc, t_vx, jj, cl.c0);
             dyy[r] = ybwd2<false, false, P, FDOH>(hc, t_vy, jj, cl.c0);
+            if (fsurf && ti.j0 + jj == 1) vys = ybwd2<false, false, P, FDOH, true>(hc, t_vy, jj, cl.c0);
 #pragma unroll
             for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
         }
@@ -694,6 +787,9 @@ struct OpSEl {
                 o[0][e] = (float)((D)sxx0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vxx)));
                 o[1][e] = (float)((D)syy0 + ((D)(gg * (vxx + vyy)) + ((D)2 * (D)f * (D)vyy)));
             }
+            if (fps && j >= src_j0 && j <= src_j1) psource_row(g, src, slot, nt, j, cl, o[0], o[1]);
+            if (fsurf && j == 1)
+                surface_row<FDOH, P::HE, 0>(g, S, M, hc, wx[r], vys, cl, slot, ti.model, o[0], o[1], nullptr, nullptr);
             const RowOut out(g, S, so, slot, j, cl);
             out.put(S.off[P_SXX], o[0][0], o[0][1]);
             out.put(S.off[P_SYY], o[1][0], o[1][1]);
