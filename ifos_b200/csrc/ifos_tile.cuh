@@ -524,6 +524,27 @@ __device__ __forceinline__ void surface_row(const KGrid &g, const KState<float> 
     }
 }
 
+// By-value forms of the two for out-of-line calls from the viscoelastic
+// stress op: its rarely taken source and surface rows then do not add to the
+// register budget of its main path (the elastic op has room and inlines them).
+template <int LL>
+struct RowVals {
+    float sxx[2], syy[2], p[LL > 0 ? LL : 1][2], q[LL > 0 ? LL : 1][2];
+};
+__device__ __noinline__ float4 psource_row_v(const KGrid &g, const KSrc &src, int slot, int nt, int j, Cols cl,
+                                             float4 v) {
+    float sxx[2] = {v.x, v.y}, syy[2] = {v.z, v.w};
+    psource_row(g, src, slot, nt, j, cl, sxx, syy);
+    return make_float4(sxx[0], sxx[1], syy[0], syy[1]);
+}
+template <int FDOH, int HE, int LL>
+__device__ __noinline__ RowVals<LL> surface_row_v(const KGrid &g, const KState<float> &S, const KModel<float> &M,
+                                                  Hc<FDOH> hc, XWin<HE> wx, float2 vy2, Cols cl, int slot, int model,
+                                                  RowVals<LL> v) {
+    surface_row<FDOH, HE, LL>(g, S, M, hc, wx, vy2, cl, slot, model, v.sxx, v.syy, v.p, v.q);
+    return v;
+}
+
 // Interior tiles take rows<false>; tiles with a strip cell rows<true>.
 // The path is chosen per warp (all lanes take the same one, so that the
 // warp-wide operations of the snapshot store and the stage release meet):
@@ -685,10 +706,34 @@ struct OpSVisc {
                 o[1][e] = s_yy + (dthalbe * sumq);
                 o[2][e] = s_xy + (dthalbe * sumr);
             }
-            if (fps && j >= src_j0 && j <= src_j1) psource_row(g, src, slot, nt, j, cl, o[0], o[1]);
-            if (fsurf && j == 1)
-                surface_row<FDOH, P::HE, LL>(g, S, M, hc, wx[r], vys, cl, slot, ti.model, o[0], o[1], &o[3 + LL],
-                                             &o[3 + 2 * LL]);
+            if (fps && j >= src_j0 && j <= src_j1) {
+                const float4 r4 = psource_row_v(g, src, slot, nt, j, cl, make_float4(o[0][0], o[0][1], o[1][0], o[1][1]));
+                o[0][0] = r4.x, o[0][1] = r4.y, o[1][0] = r4.z, o[1][1] = r4.w;
+            }
+            if (fsurf && j == 1) {
+                RowVals<LL> rv;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    rv.sxx[e] = o[0][e];
+                    rv.syy[e] = o[1][e];
+#pragma unroll
+                    for (int l = 0; l < LL; l++) {
+                        rv.p[l][e] = o[3 + LL + l][e];
+                        rv.q[l][e] = o[3 + 2 * LL + l][e];
+                    }
+                }
+                rv = surface_row_v<FDOH, P::HE, LL>(g, S, M, hc, wx[r], vys, cl, slot, ti.model, rv);
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    o[0][e] = rv.sxx[e];
+                    o[1][e] = rv.syy[e];
+#pragma unroll
+                    for (int l = 0; l < LL; l++) {
+                        o[3 + LL + l][e] = rv.p[l][e];
+                        o[3 + 2 * LL + l][e] = rv.q[l][e];
+                    }
+                }
+            }
             const RowOut out(g, S, so, slot, j, cl);
             out.put(S.off[P_SXX], o[0][0], o[0][1]);
             out.put(S.off[P_SYY], o[1][0], o[1][1]);
