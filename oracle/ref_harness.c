@@ -6,9 +6,10 @@
  * reference driver.  This file contains no propagation arithmetic of its own:
  * it allocates the reference's NR-style arrays (util.c), sets the reference's
  * global scalars (globvar.h, compiled from the reference tree), and calls
- *   setup   matcopy_elastic/matcopy, av_mue, av_rho, av_tau,
- *           prepare_update_s, PML_pro, holbergcoeff   (src/IFOS2D.c:773-943)
- *   forward update_v_PML(_SH), update_s_*_PML(_SH), psource, surface_*,
+ *   setup   matcopy_elastic/matcopy/matcopy_viscac, av_mue, av_rho, av_tau,
+ *           prepare_update_s/_p, PML_pro, holbergcoeff (src/IFOS2D.c:773-943)
+ *   forward update_v_PML(_SH), update_s_*_PML(_SH), update_p(_visc)_PML,
+ *           psource, surface_*,
  *           seismo_ssg, snapshot store               (src/IFOS2D.c:1651-1894)
  *   adjoint the same kernels with sw=1 + zero-lag correlation
  *                                                    (src/IFOS2D.c:2224-2438)
@@ -195,7 +196,7 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
 
     /* material ghost ring + averages (src/IFOS2D.c:906-943) */
     if (L && !ACOUSTIC) matcopy(prho, ppi, pu, ptaus, ptaup);
-    else if (!ACOUSTIC) matcopy_elastic(prho, ppi, pu);
+    else if (L) matcopy_viscac(prho, ppi, ptaup);
     else matcopy_elastic(prho, ppi, pu);
     if (!ACOUSTIC) av_mue(pu, puipjp, prho);
     av_rho(prho, prip, prjp);
@@ -203,6 +204,8 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
     if (L && !ACOUSTIC)
         prepare_update_s(etajm, etaip, peta, fipjp, pu, puipjp, ppi, prho, ptaus, ptaup, ptausipjp, f, g,
                          bip, bjm, cip, cjm, dip, d, e);
+    else if (L)
+        prepare_update_p(etajm, peta, ppi, prho, ptaup, g, bjm, cjm, e);
 
     /* CPML profiles (src/IFOS2D.c:816) */
     int n2 = 2 * FW > 0 ? 2 * FW : 1;
@@ -302,6 +305,10 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
                                   hc, 0, pr, pp, pq, fipjp, f, g, bip, bjm, cip, cjm, d, e, dip, K_x, a_x, b_x,
                                   K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half, psi_vxx,
                                   psi_vyy, psi_vxy, psi_vyx);
+            if (psv && ACOUSTIC)
+                update_p_visc_PML(1, NX, 1, NY, pvx, pvy, psp, ppi, prho, hc, 0, pp, g, bjm, cjm, e, K_x, a_x, b_x,
+                                  K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half, psi_vxx,
+                                  psi_vyy, psi_vxy, psi_vyx);
             if (sh)
                 update_s_visc_PML_SH(1, NX, 1, NY, pvz, psxz, psyz, pt, po, bip, bjm, cip, cjm, d, dip, fipjp, f, hc,
                                      0, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half,
@@ -393,7 +400,10 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
             srcpos_loc_back[2][i] = recpos_loc[2][i];
         }
         /* zero wavefields (src/IFOS2D.c:2193-2213) */
-        if (L)
+        if (L && ACOUSTIC)
+            zero_fdveps_viscac(-nd + 1, NY + nd, -nd + 1, NX + nd, pvx, pvy, psp, pvxp1, pvyp1, psi_sxx_x, psi_sxy_x,
+                               psi_vxx, psi_vyx, psi_syy_y, psi_sxy_y, psi_vyy, psi_vxy, psi_vxxs, pp);
+        else if (L)
             zero_fdveps_visc(-nd + 1, NY + nd, -nd + 1, NX + nd, pvx, pvy, pvz, psxx, psyy, psxy, psxz, psyz, ux, uy,
                              uxy, pvxp1, pvyp1, psi_sxx_x, psi_sxy_x, psi_sxz_x, psi_vxx, psi_vyx, psi_vzx, psi_syy_y,
                              psi_sxy_y, psi_syz_y, psi_vyy, psi_vxy, psi_vzy, psi_vxxs, pr, pp, pq, pt, po);
@@ -425,6 +435,10 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
                 if (psv && !ACOUSTIC)
                     update_s_visc_PML(1, NX, 1, NY, pvx, pvy, ux, uy, uxy, uyx, psxx, psyy, psxy, ppi, pu, puipjp,
                                       prho, hc, 0, pr, pp, pq, fipjp, f, g, bip, bjm, cip, cjm, d, e, dip, K_x, a_x,
+                                      b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
+                                      psi_vxx, psi_vyy, psi_vxy, psi_vyx);
+                if (psv && ACOUSTIC)
+                    update_p_visc_PML(1, NX, 1, NY, pvx, pvy, psp, ppi, prho, hc, 0, pp, g, bjm, cjm, e, K_x, a_x,
                                       b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
                                       psi_vxx, psi_vyy, psi_vxy, psi_vyx);
                 if (sh)

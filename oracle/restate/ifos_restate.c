@@ -288,6 +288,7 @@ static void setup_model(const grid_t *g, shot_t *s, const orc_shot_io *io) {
     ghost_ring(g, s->vp);
     ghost_ring(g, s->vs);
     if (L && !c->acoustic) { ghost_ring(g, s->taus); ghost_ring(g, s->taup); }
+    if (L && c->acoustic) ghost_ring(g, s->taup); /* src/matcopy_viscac.c: rho, pi, taup */
     /* harmonic shear modulus at (i+1/2, j+1/2), src/av_mue.c:45-61 */
     if (!c->acoustic)
         for (int j = 1; j <= NY; j++)
@@ -306,14 +307,16 @@ static void setup_model(const grid_t *g, shot_t *s, const orc_shot_io *io) {
             A(s->rjp, j, i) = 1.0 / (0.5 * (A(s->rho, j, i) + A(s->rho, j + 1, i)));
             A(s->rip, j, i) = 1.0 / (0.5 * (A(s->rho, j, i) + A(s->rho, j, i + 1)));
         }
-    if (!L || c->acoustic) return;
-    /* src/av_tau.c:25-29 */
+    if (!L) return;
+    /* src/av_tau.c:25-29 (unused by the acoustic update) */
     for (int j = 1; j <= NY; j++)
         for (int i = 1; i <= NX; i++)
             A(s->tausipjp, j, i) =
                 0.25 * (A(s->taus, j, i) + A(s->taus, j, i + 1) + A(s->taus, j + 1, i) + A(s->taus, j + 1, i + 1));
-    /* relaxation: eta_l = DT*2*pi*FL_l (src/readmod.c:44-49), then the
-     * coefficient set of src/prepare_update_s.c:33-77 */
+    /* relaxation: eta_l = DT*2*pi*FL_l (src/readmod.c:44-49,
+     * src/readmod_viscac.c:47-50), then the coefficient set of
+     * src/prepare_update_s.c:33-77; the acoustic set of
+     * src/prepare_update_p.c:44-64 (g, bjm, cjm, e) is the same formulas */
     float pts[ORC_MAX_L + 1];
     for (int l = 1; l <= L; l++) {
         pts[l] = 1.0 / (2.0 * PI_D * c->fl[l - 1]);
@@ -725,6 +728,43 @@ static void update_p_ac(const grid_t *g, shot_t *s) {
         }
 }
 
+/* viscoacoustic pressure with L relaxation mechanisms:
+ * src/update_p_visc_PML.c:61-146 (FDORDER 2: written-out differences and
+ * CPML, whose vyx/vxy memories it also advances) and :148-182 (every other
+ * order: the generic loop from zero, without CPML) */
+static void update_p_visc(const grid_t *g, shot_t *s) {
+    const float DT = g->c.dt, DH = g->c.dh;
+    const float dhi = 1.0 / DH, dthalbe = DT / 2.0;
+    const int L = g->c.L;
+    for (int j = 1; j <= g->ny; j++)
+        for (int i = 1; i <= g->nx; i++) {
+            float vxx, vyy;
+            if (g->c.fdorder == 2) {
+                vxx = dfx_bwd(g, s->vx, j, i) * dhi;
+                float vyx = dfx_fwd(g, s->vy, j, i) * dhi;
+                float vxy = dfy_fwd(g, s->vx, j, i) * dhi;
+                vyy = dfy_bwd(g, s->vy, j, i) * dhi;
+                CPML_X(s->psi_vxx, j, i, g->bx, g->ax, g->Kx, vxx);
+                CPML_X(s->psi_vyx, j, i, g->bxh, g->axh, g->Kxh, vyx);
+                CPML_Y(s->psi_vyy, j, i, g->by, g->ay, g->Ky, vyy);
+                CPML_Y(s->psi_vxy, j, i, g->byh, g->ayh, g->Kyh, vxy);
+            } else {
+                vxx = dfx_bwd_z(g, s->vx, j, i) * dhi;
+                vyy = dfy_bwd_z(g, s->vy, j, i) * dhi;
+            }
+            float sump = 0.0f;
+            for (int l = 1; l <= L; l++) sump += A(s->p[l], j, i);
+            A(s->sp, j, i) += (A(s->g, j, i) * (vxx + vyy)) + (dthalbe * sump);
+            sump = 0.0f;
+            for (int l = 1; l <= L; l++) {
+                float *pp = &A(s->p[l], j, i);
+                *pp = s->bjm[l] * (*pp * s->cjm[l] - (A(s->e[l], j, i) * (vxx + vyy)));
+                sump += *pp;
+            }
+            A(s->sp, j, i) += (dthalbe * sump);
+        }
+}
+
 /* explosive source (forward) / pressure residual (adjoint, ADJOINT_TYPE 4),
  * src/psource.c:37-74 */
 static void psource(const grid_t *g, shot_t *s, int nt, int n, const float *pos, const float *sig, int sw) {
@@ -879,6 +919,8 @@ static void step(const grid_t *g, shot_t *s, int nt, int sw, const orc_shot_io *
     if (!c->acoustic) {
         if (g->psv) { if (c->L) update_s_psv_visc(g, s); else update_s_psv_el(g, s); }
         if (g->sh) update_s_sh(g, s);
+    } else if (c->L) {
+        update_p_visc(g, s);
     } else {
         update_p_ac(g, s);
     }

@@ -22,6 +22,9 @@ CASES = {
     # CPML with K profiles above 1 (k_max_PML > 1): the d/K division of the recursion
     "psv_visc_o4_kmax2": dict(L=3, fl=FL, tau=TAU, f_ref=40.0, k_max_pml=2.0),
     "sh_el_o4_kmax3": dict(wavetype=2, k_max_pml=3.0, free_surf=0),
+    # viscoacoustic pressure (src/update_p_visc_PML.c): CPML only at FDORDER 2
+    "ac_visc_o2_nofs": dict(acoustic=1, L=2, fl=FL[:2], tau=TAU, f_ref=40.0, fdorder=2, free_surf=0),
+    "ac_visc_o4_p": dict(acoustic=1, L=3, fl=FL, tau=TAU, f_ref=40.0, seismo=2, adjoint_type=4),
 }
 
 

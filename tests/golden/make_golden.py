@@ -4,7 +4,7 @@ by oracle/Makefile from the IFOS2D source tree) are run on small seeded cases
 and their outputs are stored here.  Run in a container that has the
 reference tree:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   (all cases and the set-up file when none are named)
 
 The fixtures pin the C restatement (oracle/liboracle.so) bit-for-bit on
 machines without the reference tree.
@@ -22,14 +22,16 @@ from oracle import oracle as O  # noqa: E402
 from tests.golden.cases import CASES, build_case  # noqa: E402
 
 
-def main():
+def main(names=None):
     O.build("ref")
-    for name in CASES:
+    for name in names or CASES:
         p, model, g, sig, adj = build_case(name)
         out = O.run_shot("ref", p, model, g.srcpos, sig, g.recpos, run_adjoint=True, adj=adj)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), sections=out["sections"], fields=out["fields"],
                             grads=out["grads"], adj_fields=out["adj_fields"])
         print(name, {k: float(np.linalg.norm(v)) for k, v in out.items()})
+    if names:
+        return
     # set-up functions
     p, model, g, sig, adj = build_case("psv_el_o4")
     prof = {f"pml_fw{fw}": O.pml_profiles("ref", p.copy(fw=fw, npower=npw, vppml=v))
@@ -46,4 +48,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -19,6 +19,9 @@ CONFIGS = [
     dict(fdorder=2, acoustic=1, seismo=5, maxrelerror=2),
     dict(fdorder=4, adjoint_type=3, boundary=1),
     dict(fdorder=4, adjoint_type=2, source_type=4),
+    # viscoacoustic: FDORDER 2 (CPML) and a generic-loop order (no CPML)
+    dict(fdorder=2, acoustic=1, L=2, fl=FL[:2], tau=TAU, f_ref=20.0, free_surf=0),
+    dict(fdorder=6, acoustic=1, L=3, fl=FL, tau=TAU, f_ref=20.0, seismo=2, adjoint_type=4),
 ]
 
 
