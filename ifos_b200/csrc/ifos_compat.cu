@@ -759,6 +759,42 @@ __global__ void kc_p(RG g, Prof P, const float *vx, const float *vy, float *sp, 
     if (u) u[c] = (gg / DT) * (vxx + vyy);
 }
 
+// update_p_visc_PML (src/update_p_visc_PML.c:61-146 at FDORDER 2, with CPML
+// on all four velocity derivatives; :148-182 for every other order, the
+// generic loop from zero without CPML)
+template <int FD>
+__global__ void kc_p_visc(RG g, Prof P, const float *vx, const float *vy, float *sp, float *p, const float *gv,
+                          const float *bjm, const float *cjm, const float *e, float *ps_vxx, float *ps_vyy,
+                          float *ps_vxy, float *ps_vyx) {
+    CELL_IJ(g)
+    constexpr bool Z0 = FD != 1;
+    const long long s = g.stride;
+    const float DT = g.dt, DH = g.dh;
+    const float dhi = 1.0 / DH, dthalbe = DT / 2.0;  // src/update_p_visc_PML.c:49-51
+    float vxx = sbwd<FD, Z0>(g, vx, c, 1) * dhi;
+    float vyy = sbwd<FD, Z0>(g, vy, c, s) * dhi;
+    if (FD == 1 && ps_vxx) {
+        float vyx = sfwd<FD, false>(g, vy, c, 1) * dhi;
+        float vxy = sfwd<FD, false>(g, vx, c, s) * dhi;
+        vxx = pmlx(g, P, ps_vxx, j, i, PK_X, PA_X, PB_X, vxx);
+        vyx = pmlx(g, P, ps_vyx, j, i, PK_XH, PA_XH, PB_XH, vyx);
+        vyy = pmly(g, P, ps_vyy, j, i, PK_Y, PA_Y, PB_Y, vyy);
+        vxy = pmly(g, P, ps_vxy, j, i, PK_YH, PA_YH, PB_YH, vxy);
+        (void)vyx, (void)vxy;
+    }
+    const int L = g.L;
+    const long long t0 = c * L;
+    float sump = 0.0f;
+    for (int l = 0; l < L; l++) sump += p[t0 + l];
+    sp[c] += (gv[c] * (vxx + vyy)) + (dthalbe * sump);
+    sump = 0.0f;
+    for (int l = 0; l < L; l++) {
+        p[t0 + l] = bjm[l] * (p[t0 + l] * cjm[l] - (e[t0 + l] * (vxx + vyy)));
+        sump += p[t0 + l];
+    }
+    sp[c] += (dthalbe * sump);
+}
+
 // surface_acoustic_PML (src/surface_acoustic_PML.c:36-42): zero at the
 // surface, imaged above it
 __global__ void kc_surf_ac(RG g, int j, float *sp) {
@@ -1429,6 +1465,46 @@ extern "C" void update_p_PML(int nx1, int nx2, int ny1, int ny2, float **vx, flo
     if (pml) {
         down(pblk(psi_vxx), psix_bytes());
         down(pblk(psi_vyy), psiy_bytes());
+    }
+    finish();
+}
+
+extern "C" void update_p_visc_PML(int nx1, int nx2, int ny1, int ny2, float **vx, float **vy, float **sp,
+                                  float **pi, float **rho, float *hc, int infoout, float ***p, float **g_, float *bjm,
+                                  float *cjm, float ***e, float *K_x, float *a_x, float *b_x, float *K_x_half,
+                                  float *a_x_half, float *b_x_half, float *K_y, float *a_y, float *b_y,
+                                  float *K_y_half, float *a_y_half, float *b_y_half, float **psi_vxx,
+                                  float **psi_vyy, float **psi_vxy, float **psi_vyx) {
+    (void)pi, (void)rho, (void)infoout;
+    const size_t fb = field_bytes(), tb = tensor_bytes();
+    const RG g = make_rg(nx1, nx2, ny1, ny2, hc);
+    const bool pml = FDORDER == 2 && FW > 0;
+    const float *d_vx = up(fblk(vx), fb), *d_vy = up(fblk(vy), fb);
+    float *d_sp = up(fblk(sp), fb), *d_p = up(tblk(p), tb);
+    const float *d_g = up(fblk(g_), fb), *d_e = up(tblk(e), tb);
+    const float *d_bjm = vec_up(bjm), *d_cjm = vec_up(cjm);
+    float *ps[4] = {nullptr, nullptr, nullptr, nullptr};
+    Prof P{nullptr, 2 * FW};
+    if (pml) {
+        ps[0] = up(pblk(psi_vxx), psix_bytes());
+        ps[1] = up(pblk(psi_vyy), psiy_bytes());
+        ps[2] = up(pblk(psi_vxy), psiy_bytes());
+        ps[3] = up(pblk(psi_vyx), psix_bytes());
+        float *const pv[12] = {K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half};
+        P = upload_prof(pv);
+    }
+    if (nx2 >= nx1 && ny2 >= ny1) {
+        const dim3 gr = grid_of(nx1, nx2, ny1, ny2);
+        DISPATCH_FD(g.fdoh, kc_p_visc<FD><<<gr, kBlk, 0, stream()>>>(g, P, d_vx, d_vy, d_sp, d_p, d_g, d_bjm, d_cjm, d_e, ps[0], ps[1], ps[2], ps[3]));
+        check_launch("update_p_visc_PML");
+    }
+    down(fblk(sp), fb);
+    down(tblk(p), tb);
+    if (pml) {
+        down(pblk(psi_vxx), psix_bytes());
+        down(pblk(psi_vyy), psiy_bytes());
+        down(pblk(psi_vxy), psiy_bytes());
+        down(pblk(psi_vyx), psix_bytes());
     }
     finish();
 }

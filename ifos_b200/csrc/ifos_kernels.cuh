@@ -522,6 +522,51 @@ __global__ void k_p_ac(KGrid g, KState<T> S, KModel<T> M) {
     sp[c] += modelp(M, slot, M_GAC)[c] * (vxx + vyy);
 }
 
+// pressure half step, viscoacoustic with L relaxation mechanisms
+// (src/update_p_visc_PML.c: FDORDER 2 :61-146 with CPML; every other order
+// :148-182, sums from zero and no CPML).  The CPML memories of vyx and vxy
+// that its FDORDER 2 branch also advances feed nothing else and are not kept.
+template <typename T, int FDOH>
+__global__ void k_p_visc(KGrid g, KState<T> S, KModel<T> M) {
+    constexpr bool Z0 = FDOH != 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int slot = blockIdx.z;
+    if (i > g.nx || j > g.ny) return;
+    const T *vx = fieldp(S, slot, P_VX), *vy = fieldp(S, slot, P_VY);
+    T *sp = fieldp(S, slot, P_SP);
+    const long long c = pidx(g, j, i);
+    const T DT = g.dt, DH = g.dh;
+    const T dhi = (T)(1.0 / (double)DH), dthalbe = (T)((double)DT / 2.0);
+    T vxx = 0, vyy = 0;
+#pragma unroll
+    for (int m = 1; m <= FDOH; m++) vxx = tap(m, vxx, (T)g.hc[m] * (vx[pidx(g, j, i + m - 1)] - vx[pidx(g, j, i - m)]), Z0);
+#pragma unroll
+    for (int m = 1; m <= FDOH; m++) vyy = tap(m, vyy, (T)g.hc[m] * (vy[pidx(g, j + m - 1, i)] - vy[pidx(g, j - m, i)]), Z0);
+    vxx = vxx * dhi;
+    vyy = vyy * dhi;
+    if (FDOH == 1) {
+        vxx = cpml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, i, K_X, A_X, B_X, vxx);
+        vyy = cpml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, j, i, K_Y, A_Y, B_Y, vyy);
+    }
+    const int L = g.L;
+    T sump = 0;
+    for (int l = 1; l <= L; l++) sump += memp(S, g, slot, 1, l)[c];
+    const T gg = modelp(M, slot, M_GV)[c], pi = modelp(M, slot, M_PIR)[c];
+    const T *tpp = modelp(M, slot, M_TAUP);
+    const T tp = tpp ? tpp[c] : (T)g.taup0;
+    sp[c] += (gg * (vxx + vyy)) + (dthalbe * sump);
+    sump = 0;
+    for (int l = 1; l <= L; l++) {
+        const T e = pi * (T)g.eta[l] * tp;  // e of src/prepare_update_p.c:62, formed in the same order
+        T *pp = memp(S, g, slot, 1, l) + c;
+        const T p = (T)g.bjm[l] * (*pp * (T)g.cjm[l] - (e * (vxx + vyy)));
+        *pp = p;
+        sump += p;
+    }
+    sp[c] += (dthalbe * sump);
+}
+
 // Cells of a snapshot that the stencil kernels stored and a later kernel of
 // the same step changes (explosive sources, the free surface): base of the
 // snapshot of slot 0 being stored (NULL: nothing to patch), floats between

@@ -187,6 +187,25 @@ bool build_model(const ifos_params &p, const float *vp, const float *vs, const f
     if (p.acoustic) {
         o.g_ac.resize(N);
         for (size_t k = 0; k < N; k++) o.g_ac[k] = R[k] * (PI[k] * PI[k]);  // src/update_p_PML.c:98
+        if (!p.L) return true;
+        // viscoacoustic (src/prepare_update_p.c:44-64): the relaxed modulus pi
+        // and g = pi*DT*(1+L*taup); e_l = pi*eta_l*taup is formed in the kernels
+        const ViscoScalars vs_ = visco_scalars(p);
+        std::vector<float> tp(N);
+        for (size_t k = 0; k < N; k++) tp[k] = taup ? taup[k] : p.tau;
+        o.g_v.resize(N);
+        o.pi_r.resize(N);
+        for (size_t k = 0; k < N; k++) {
+            float pi = (PI[k] * PI[k] * R[k]) / (1.0 + vs_.sumpi * tp[k]);
+            o.g_v[k] = pi * p.dt * (1.0 + p.L * tp[k]);
+            o.pi_r[k] = pi;
+        }
+        o.tau_uniform = true;
+        for (size_t k = 1; k < N && o.tau_uniform; k++)
+            if (tp[k] != tp[0]) o.tau_uniform = false;
+        o.taus0 = o.tausipjp0 = 0.0f;
+        o.taup0 = tp[0];
+        if (!o.tau_uniform) o.taup = tp;
         return true;
     }
     o.uipjp.resize(N);

@@ -249,7 +249,6 @@ static int check_params(const ifos_params &p, std::string &why) {
     if (p.L < 0 || p.L > IFOS_MAX_L) return bad("L must be 0..8");
     if (p.wavetype < 1 || p.wavetype > 3) return bad("WAVETYPE must be 1, 2 or 3");
     if (p.acoustic && p.wavetype != 1) return bad("acoustic modelling is P-SV only");
-    if (p.acoustic && p.L) return bad("viscoacoustic modelling is not implemented on the device");
     if (p.parameterization != 1) return bad("only PARAMETERIZATION=1 is implemented");
     if (p.velocity != 0) return bad("only VELOCITY=0 is implemented");
     if (p.dtinv < 1 || p.nt % p.dtinv) return bad("NT must be a multiple of DTINV");
@@ -281,14 +280,14 @@ static Layout layout_of(const ifos_params &p) {
     L.nfield = 0;
     if (psv) L.nfield += p.acoustic ? 5 : 7;
     if (sh) L.nfield += 4;
-    L.nmem = p.L ? (psv ? 3 * p.L : 0) + (sh ? 2 * p.L : 0) : 0;
+    L.nmem = p.L ? (psv ? (p.acoustic ? 1 : 3) * p.L : 0) + (sh ? 2 * p.L : 0) : 0;
     L.slot_elems = (long long)(L.nfield + L.nmem) * L.plane;
     L.psix = (long long)p.ny * 2 * p.fw;
     L.psiy = (long long)2 * p.fw * p.nx;
     L.psi_slot = NX_STRIP * L.psix + NY_STRIP * L.psiy;
     // model planes: rho vp vs rip rjp always; + elastic (uipjp f g mm ll) or acoustic g;
-    // + visco (fipjp f g mu pi muipjp [taus taup tausipjp])
-    L.nmodel = 5 + (p.acoustic ? 1 : 5) + (p.L ? 9 : 0);
+    // + visco (fipjp f g mu pi muipjp [taus taup tausipjp]) or viscoacoustic (g pi [taup])
+    L.nmodel = 5 + (p.acoustic ? 1 : 5) + (p.L ? (p.acoustic ? 3 : 9) : 0);
     L.model_elems = (long long)L.nmodel * L.plane;
     L.ncomp = (psv ? (p.acoustic ? 3 : 5) : 0) + (sh ? 3 : 0);
     const int bytes = p.snap_format == 0 ? (p.precision ? 8 : 4) : 2;
@@ -522,6 +521,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     if (p.L) {
         if (c->psv)
             for (int w = 0; w < 3; w++) {
+                if (c->ac && w != 1) continue;  // viscoacoustic: the pressure memories only
                 c->mem_off[w] = k * L.plane;
                 k += p.L;
             }
@@ -629,7 +629,9 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
         present.push_back(M_MM);
         present.push_back(M_LL);
     }
-    if (p.L)
+    if (p.L && c->ac)
+        for (int m : {M_GV, M_PIR, M_TAUP}) present.push_back(m);
+    else if (p.L)
         for (int m : {M_FIPJPV, M_FV, M_GV, M_MUR, M_PIR, M_MUIPJPR, M_TAUS, M_TAUP, M_TAUSIPJP}) present.push_back(m);
     for (size_t q = 0; q < present.size(); q++) {
         c->mplane[present[q]] = true;
@@ -961,12 +963,26 @@ struct Launcher {
         }
         if (c->sh) pipelined(OpSSh<FD, kTileY, LL, ring_stages<FD, 1, 2 + 2 * LL + 4, 0>()>{g, S, M, c->ktma, snap_out(hin)});
     }
+    template <int FD, int LL>
+    void p_visc_pipe(int hin) {
+        pipelined(OpPVisc<FD, kTileY, LL, ring_stages<FD, 2, 3 + LL, 0>()>{c->g, S, M, c->ktma, snap_out(hin)});
+    }
     template <int FD>
     void s_pipe(int hin) {
         const KGrid &g = c->g;
         const KTma &t = c->ktma;
         bool quirk = false;
         if constexpr (FD >= 5) quirk = g.quirk_hi != 0;
+        if (c->ac && g.L) {
+            switch (g.L) {
+                case 1: p_visc_pipe<FD, 1>(hin); break;
+                case 2: p_visc_pipe<FD, 2>(hin); break;
+                case 3: p_visc_pipe<FD, 3>(hin); break;
+                case 4: p_visc_pipe<FD, 4>(hin); break;
+                default: p_visc_pipe<FD, 5>(hin); break;
+            }
+            return;
+        }
         if (c->ac) {
             constexpr int NST = ring_stages<FD, 2, 2, 0>();
             if constexpr (FD >= 5) {
@@ -1028,7 +1044,8 @@ struct Launcher {
             }
         }
         DISPATCH_FDOH(g.fdoh, {
-            if (c->ac) k_p_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+            if (c->ac && g.L) k_p_visc<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
+            else if (c->ac) k_p_ac<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);
             else {
                 if (c->psv) {
                     if (g.L) k_s_psv_visc<T, FD><<<grd, blk, 0, c->st>>>(g, S, M);

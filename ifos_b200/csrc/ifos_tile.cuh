@@ -1252,6 +1252,91 @@ struct OpPAc {
         }
     }
 };
+// pressure, viscoacoustic with LL relaxation mechanisms
+// (src/update_p_visc_PML.c:61-146 at FDORDER 2, with CPML; :148-182 for every
+// other order: sums from zero and no CPML, hence Z0 and no strip path)
+// halo: vx vy; plain: sp p[LL] g pi; writes sp p[LL].  Non-uniform taup is
+// read from HBM.
+template <int FDOH, int TY, int LL, int NST>
+struct OpPVisc {
+    static constexpr bool Z0 = FDOH != 1;
+    static constexpr int NH_ = 2, NP_ = 3 + LL;
+    using P = Pipe<FDOH, TY, NH_, NP_, 0, NST>;
+    IFOS_OP_MEMBERS
+    __device__ void planes(const TileInfo &ti, int *hz, PlainSrc *pz) const {
+        const int zb = ti.slot * tm.planes_per_slot;
+        const int mb = ti.model * tm.model_planes;
+        hz[0] = zb + tm.pid[P_VX];
+        hz[1] = zb + tm.pid[P_VY];
+        pz[0] = {zb + tm.pid[P_SP], false};
+#pragma unroll
+        for (int l = 0; l < LL; l++) pz[1 + l] = {zb + tm.mem_pid[1] + l, false};
+        pz[1 + LL] = {mb + tm.mid[M_GV], true};
+        pz[2 + LL] = {mb + tm.mid[M_PIR], true};
+    }
+    IFOS_TILE_COMPUTE(Z0)
+    template <bool PML>
+    __device__ __forceinline__ void rows(const TileInfo &ti, const Cols &cl, const float *h, const float *pl,
+                                         uint64_t *empty) const {
+        constexpr int RT = P::RT;
+        const float *t_vx = h, *t_vy = h + P::BOXS;
+        const Hc<FDOH> hc(g);
+        XWin<P::HE> wx[RT];
+        float2 dyy[RT], in[RT][NP_];
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int jj = threadIdx.y * RT + r;
+            wx[r].load(t_vx + (jj + P::H) * P::BW, cl.c0);
+            dyy[r] = ybwd2<false, false, P, FDOH, Z0>(hc, t_vy, jj, cl.c0);
+#pragma unroll
+            for (int q = 0; q < NP_; q++) in[r][q] = lds2(pl + q * P::PLS + jj * kTileX + 2 * cl.lane);
+        }
+        release_stage(empty);
+        const int slot = ti.slot;
+        const float *tp_p = M.m[M_TAUP] ? M.m[M_TAUP] + (long long)ti.model * M.model_stride : nullptr;
+        const float DT = g.dt, DH = g.dh;
+        const float dhi = (float)(1.0 / (double)DH), dthalbe = (float)((double)DT / 2.0);
+#pragma unroll
+        for (int r = 0; r < RT; r++) {
+            const int j = ti.j0 + threadIdx.y * RT + r;
+            if (j > g.ny) break;
+            float o[1 + LL][2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const float2 *v = in[r];
+                float vxx = xbwd<FDOH, P::HE, Z0>(hc, wx[r], e) * dhi, vyy = pick(dyy[r], e) * dhi;
+                const bool ok = cl.valid(e);
+                if (PML && ok) {
+                    const int hx = cl.hx(e), ii = cl.i + e;
+                    if (hx) vxx = pml_x(g, M, S.psix[X_VXX] + slot * S.psix_slot, j, hx, K_X, A_X, B_X, vxx);
+                    const int hy = strip_y(g, j);
+                    if (hy) vyy = pml_y(g, M, S.psiy[Y_VYY] + slot * S.psiy_slot, ii, hy, K_Y, A_Y, B_Y, vyy);
+                }
+                float sump = 0;
+#pragma unroll
+                for (int l = 0; l < LL; l++) sump += pick(v[1 + l], e);
+                const float gg = pick(v[1 + LL], e), pi = pick(v[2 + LL], e);
+                float tp = g.taup0;
+                if (ok && tp_p) tp = tp_p[(j - 1 + HY) * g.pitch + (cl.i + e - 1 + HX)];
+                const float s = pick(v[0], e) + ((gg * (vxx + vyy)) + (dthalbe * sump));
+                sump = 0;
+#pragma unroll
+                for (int l = 0; l < LL; l++) {
+                    const float ee = pi * g.eta[l + 1] * tp;  // e of src/prepare_update_p.c:62
+                    const float pp = g.bjm[l + 1] * (pick(v[1 + l], e) * g.cjm[l + 1] - (ee * (vxx + vyy)));
+                    o[1 + l][e] = pp;
+                    sump += pp;
+                }
+                o[0][e] = s + (dthalbe * sump);
+            }
+            const RowOut out(g, S, so, slot, j, cl);
+            out.put(S.off[P_SP], o[0][0], o[0][1]);
+#pragma unroll
+            for (int l = 0; l < LL; l++) out.put(S.mem_off[1] + l * g.plane, o[1 + l][0], o[1 + l][1]);
+            out.snap(so.n, tm.snap_comp[P_SP], o[0][0], o[0][1]);
+        }
+    }
+};
 #undef IFOS_TILE_COMPUTE
 #undef IFOS_OP_MEMBERS
 

@@ -106,6 +106,13 @@ void update_p_PML(int nx1, int nx2, int ny1, int ny2, float **vx, float **vy, fl
                   float *K_y_half, float *a_y_half, float *b_y_half, float **psi_vxx, float **psi_vyy,
                   float **psi_vxy, float **psi_vyx);
 
+/* src/fd.h:556-560 (src/update_p_visc_PML.c:30) */
+void update_p_visc_PML(int nx1, int nx2, int ny1, int ny2, float **vx, float **vy, float **sp, float **pi,
+                       float **rho, float *hc, int infoout, float ***p, float **g, float *bjm, float *cjm, float ***e,
+                       float *K_x, float *a_x, float *b_x, float *K_x_half, float *a_x_half, float *b_x_half,
+                       float *K_y, float *a_y, float *b_y, float *K_y_half, float *a_y_half, float *b_y_half,
+                       float **psi_vxx, float **psi_vyy, float **psi_vxy, float **psi_vyx);
+
 /* src/fd.h:515 (src/surface_acoustic_PML.c:23) */
 void surface_acoustic_PML(int ndepth, float **sp);
 

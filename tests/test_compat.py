@@ -378,6 +378,36 @@ def test_update_p_PML(fdorder, free_surf):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fdorder,free_surf,L,rng_kind", [(2, 1, 2, "full"), (2, 0, 1, "part"), (4, 1, 3, "full"),
+                                                          (12, 0, 2, "full")])
+def test_update_p_visc_PML(fdorder, free_surf, L, rng_kind):
+    """The viscoacoustic pressure: CPML on all four velocity derivatives at
+    FDORDER 2 (the vyx / vxy memories are written back too), the generic
+    loop without CPML otherwise."""
+    g = _base(fdorder, free_surf, L=L, ACOUSTIC=1)
+    pair = H.Pair(g, 140 + fdorder + L)
+    for n in ("vx", "vy", "sp", "pi", "rho"):
+        pair.field(n)
+    pair.field("g", 0.1, 2.0)
+    pair.tensor("p")
+    pair.tensor("e", 0.0, 0.3)
+    for n in ("bjm", "cjm"):
+        pair.vec(n, pair.rng.uniform(0.5, 1.0, L))
+    for n, kind in (("psi_vxx", "x"), ("psi_vyy", "y"), ("psi_vxy", "y"), ("psi_vyx", "x")):
+        pair.psix(n) if kind == "x" else pair.psiy(n)
+    pair.profiles()
+    pair.vec("hc", HC[1:])
+    x1, x2, y1, y2 = _range(rng_kind)
+
+    def args(s):
+        P = lambda n: pair.p(s, n)
+        return [x1, x2, y1, y2, P("vx"), P("vy"), P("sp"), P("pi"), P("rho"), P("hc"), 0, P("p"), P("g"), P("bjm"),
+                P("cjm"), P("e"), *_prof(pair, s), P("psi_vxx"), P("psi_vyy"), P("psi_vxy"), P("psi_vyx")]
+
+    _run(pair, "update_p_visc_PML", args)
+
+
+@pytest.mark.gpu
 def test_surface_acoustic_PML():
     g = _base(6, 1, ACOUSTIC=1)
     pair = H.Pair(g, 130)
