@@ -125,3 +125,81 @@ def test_time_window_matches_reference(tw_ind):
     assert np.array_equal((mask & 1) > 0, late)
     assert np.array_equal((mask & 2) > 0, early)
     assert np.array_equal(got.view(np.int32), want.view(np.int32))
+
+
+@pytest.mark.parametrize("mode,testshot", [(0, 1), pytest.param(2, 0, marks=pytest.mark.gpu),
+                                           pytest.param(1, 1, marks=pytest.mark.gpu)])
+def test_killed_trace_counts_match_count_killed_traces(tmp_path, mode, testshot):
+    """Kill table from TRKILL_FILE (and the offset rule for TRKILL_OFFSET 1/2)
+    and the killed-trace counts of src/count_killed_traces.c, run from
+    oracle/_ref, for every shot of a small survey.  The offset rule runs on
+    the device, so modes 1/2 need a GPU; mode 0 is host-only."""
+    from ifos_b200 import trkill
+    rng = np.random.default_rng(mode + 5)
+    dh = 2.5
+    ntr_glob, nsrc = 23, 6
+    rx = rng.integers(1, 300, ntr_glob).astype(np.int32)
+    ry = rng.integers(1, 40, ntr_glob).astype(np.int32)
+    sx = rng.uniform(0, 750, nsrc).astype(np.float32)
+    sy = rng.uniform(0, 100, nsrc).astype(np.float32)
+    filetab = (rng.uniform(size=(ntr_glob, nsrc)) < 0.3).astype(np.int32)
+    filetab[0, 0] = 2  # only entries equal to 1 count
+    stem = os.path.join(tempfile.mkdtemp(prefix="tk"), "kill")
+    with open(stem + ".dat", "w") as fh:
+        for r in range(ntr_glob):
+            fh.write(" ".join(str(v) for v in filetab[r]) + "\n")
+    lower, upper = 100.0, 400.0
+    # this rank's traces: every other global trace, in a shuffled order
+    local = rng.permutation(np.arange(1, ntr_glob + 1, 2)).astype(np.int32)
+
+    ref, _ = H.libs()
+    H.set_globals(DH=dh, MYID=1)
+    for name, v in (("USE_WORKFLOW", 0), ("WORKFLOW_STAGE", 0), ("TRKILL_OFFSET", mode)):
+        C.c_int.in_dll(ref, name).value = v
+    C.c_float.in_dll(ref, "TRKILL_OFFSET_LOWER").value = lower
+    C.c_float.in_dll(ref, "TRKILL_OFFSET_UPPER").value = upper
+    (C.c_char * 74).in_dll(ref, "TRKILL_FILE").value = stem.encode()
+    rp = ref.imatrix(1, 3, 1, ntr_glob)
+    rl = ref.imatrix(1, 3, 1, local.size)
+    sp = ref.matrix(1, 8, 1, nsrc)
+    for r in range(ntr_glob):
+        rp[1][r + 1], rp[2][r + 1], rp[3][r + 1] = int(rx[r]), int(ry[r]), r + 1
+    for t, n in enumerate(local):
+        rl[1][t + 1], rl[2][t + 1], rl[3][t + 1] = int(rx[n - 1]), int(ry[n - 1]), int(n)
+    for s in range(nsrc):
+        sp[1][s + 1], sp[2][s + 1] = float(sx[s]), float(sy[s])
+    f = ref.count_killed_traces
+    f.restype = None
+    f.argtypes = [C.c_int, C.c_int, C.c_int, H.IPP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                  H.FPP, H.IPP]
+    solver = _solver(dh=dh) if mode else None
+    try:
+        table = trkill.kill_table(mode, ntr_glob, nsrc, np.stack([rx, ry]), np.stack([sx, sy]), lower, upper,
+                                  path=trkill.trkill_file_name(stem), solver=solver)
+    finally:
+        if solver is not None:
+            solver.close()
+    ours = (0, 0)
+    for ishot in range(1, nsrc + 1):
+        k, kt = C.c_int(0), C.c_int(0)
+        f(local.size, testshot, ntr_glob, rl, nsrc, ishot, C.byref(k), C.byref(kt), sp, rp)
+        ours_shot = trkill.count_killed_traces(table, local, ishot, bool(testshot))
+        assert ours_shot == (k.value, kt.value), ishot
+        ours = trkill.count_killed_traces(table, local, ishot, bool(testshot), *ours)
+    assert ours[0] > 0
+
+
+def test_trkill_file_errors_like_the_reference(tmp_path):
+    """Short files and a file ending right after its last value are errors
+    (the reference's end-of-file check after every value)."""
+    from ifos_b200 import trkill
+    p = tmp_path / "k.dat"
+    p.write_bytes(b"0 1\n1 0\n")
+    assert trkill.read_trkill_file(str(p), 2, 2).tolist() == [[0, 1], [1, 0]]
+    p.write_bytes(b"0 1\n1 0")
+    with pytest.raises(ValueError):
+        trkill.read_trkill_file(str(p), 2, 2)
+    p.write_bytes(b"0 1\n1\n")
+    with pytest.raises(ValueError):
+        trkill.read_trkill_file(str(p), 2, 2)
+    assert trkill.trkill_file_name("kill") == "kill.dat"
