@@ -26,7 +26,7 @@ EXPORTS = [
     "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_dot_f64_noalloc", "ifos_last_ms", "ifos_launch_count",
     "ifos_sync", "ifos_trkill_table", "ifos_time_window", "ifos_set_option", "ifos_get_option",
     "ifos_residual_adjoint", "ifos_fetch_snapshot", "ifos_opt_step", "ifos_timedomain_filt",
-    "ifos_taper_grad_shot", "ifos_median_smooth",
+    "ifos_taper_grad_shot", "ifos_median_smooth", "ifos_mat_change_test",
 ]
 OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3}
 
@@ -49,6 +49,16 @@ class IfosParams(C.Structure):
 class IfosWindow(C.Structure):
     _fields_ = [("tw_ind", C.c_int), ("picks", C.POINTER(C.c_float)), ("gamma", C.c_float),
                 ("twl_plus", C.c_float), ("twl_minus", C.c_float)]
+
+
+class IfosMatChange(C.Structure):
+    """ifos_mat_change of include/ifos_gpu.h (field order as declared)."""
+    _fields_ = [("eps_scale", C.c_float), ("iter", C.c_int), ("itest", C.c_int), ("inv_vp_iter", C.c_int),
+                ("inv_vs_iter", C.c_int), ("inv_rho_iter", C.c_int), ("lbfgs_unnormalised", C.c_int),
+                ("vp_lower", C.c_float), ("vp_upper", C.c_float), ("vs_lower", C.c_float), ("vs_upper", C.c_float),
+                ("rho_lower", C.c_float), ("rho_upper", C.c_float), ("vp_vs_ratio", C.c_float),
+                ("limit_update", C.c_int), ("s_vp", C.c_float), ("s_vs", C.c_float), ("s_rho", C.c_float),
+                ("lbfgs_npar", C.c_int), ("vs_avg", C.c_float), ("rho_avg", C.c_float), ("vp_avg", C.c_float)]
 
 
 class IfosError(RuntimeError):
@@ -116,6 +126,8 @@ def load():
         "ifos_timedomain_filt": (C.c_int, [vp, FP, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float]),
         "ifos_taper_grad_shot": (C.c_int, [vp, C.c_int, FP, C.c_float, C.c_int, C.c_int, C.c_uint]),
         "ifos_median_smooth": (C.c_int, [vp, FP, C.c_int]),
+        "ifos_mat_change_test": (C.c_int, [vp, C.POINTER(IfosMatChange), FP, FP, FP, FP, FP, FP, FP, FP, FP, FP, FP,
+                                           FP, FP, FP, IP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

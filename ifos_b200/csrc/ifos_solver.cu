@@ -18,6 +18,7 @@
 #include "ifos_setup.h"
 #include "ifos_snap.cuh"
 #include "ifos_tile.cuh"
+#include "ifos_update.cuh"
 
 using namespace ifos;
 
@@ -1863,6 +1864,92 @@ extern "C" int ifos_taper_grad_shot(ifos_ctx *c, int nshots, const float *src_xy
         (float *)c->gout.p, N, p.nx, p.ny, planes, (const KTaperShot *)scr, (const float *)((char *)scr + tb));
     c->launches++;
     CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_mat_change_test(ifos_ctx *c, const ifos_mat_change *mc, float *vp, float *vs, float *rho,
+                                    const float *g_vp, const float *g_vs, const float *g_rho, const float *vp_start,
+                                    const float *vs_start, const float *rho_start, float *vp1, float *vs1,
+                                    float *rho1, float *s_lbfgs, float *eps, int *ratio_hit) {
+    if (!c || !mc) return IFOS_ERR_ARG;
+    const bool ac = c->ac;
+    if (!vp || !rho || !g_vp || !g_rho || !vp1 || !rho1 || (!ac && (!vs || !g_vs || !vs1)))
+        return fail(c, IFOS_ERR_ARG, "missing model, search-direction or output planes");
+    if (mc->limit_update == 1 && (!vp_start || !rho_start || (!ac && !vs_start)))
+        return fail(c, IFOS_ERR_ARG, "the limited update needs the start model");
+    KMatChange m{};
+    m.nx = c->p.nx;
+    m.ny = c->p.ny;
+    m.n = (long long)m.nx * m.ny;
+    m.acoustic = ac ? 1 : 0;
+    m.eps_scale = mc->eps_scale;
+    m.iter = mc->iter;
+    m.itest = mc->itest;
+    m.inv_vp_iter = mc->inv_vp_iter;
+    m.inv_vs_iter = mc->inv_vs_iter;
+    m.inv_rho_iter = mc->inv_rho_iter;
+    m.lbfgs_unnormalised = mc->lbfgs_unnormalised;
+    m.vp_lower = mc->vp_lower, m.vp_upper = mc->vp_upper;
+    m.vs_lower = mc->vs_lower, m.vs_upper = mc->vs_upper;
+    m.rho_lower = mc->rho_lower, m.rho_upper = mc->rho_upper;
+    m.vp_vs_ratio = mc->vp_vs_ratio;
+    m.limit_update = mc->limit_update;
+    m.s_vp = mc->s_vp, m.s_vs = mc->s_vs, m.s_rho = mc->s_rho;
+    m.lbfgs_npar = s_lbfgs ? std::max(0, std::min(3, mc->lbfgs_npar)) : 0;
+    m.vs_avg = mc->vs_avg, m.rho_avg = mc->rho_avg, m.vp_avg = mc->vp_avg;
+    CK(cudaSetDevice(c->device));
+    const long long N = m.n;
+    const size_t pb = (size_t)N * 4;
+    void *scr = nullptr;
+    if (int rc = scratch(c, 15 * pb + 64, &scr)) return rc;
+    float *d = (float *)scr;
+    float *d_vp = d, *d_vs = d + N, *d_rho = d + 2 * N, *d_gvp = d + 3 * N, *d_gvs = d + 4 * N, *d_grho = d + 5 * N;
+    float *d_vp0 = d + 6 * N, *d_vs0 = d + 7 * N, *d_rho0 = d + 8 * N;
+    float *d_vp1 = d + 9 * N, *d_vs1 = d + 10 * N, *d_rho1 = d + 11 * N, *d_s = d + 12 * N;
+    unsigned *d_mx = (unsigned *)(d + 15 * N);
+    float *d_eps = (float *)(d_mx + 8);
+    int *d_hit = (int *)(d_eps + 4);
+    auto h2d = [&](float *dst, const float *src) -> cudaError_t {
+        return src ? cudaMemcpyAsync(dst, src, pb, cudaMemcpyHostToDevice, c->st) : cudaSuccess;
+    };
+    const bool lim = mc->limit_update == 1;
+    CK(h2d(d_vp, vp));
+    CK(h2d(d_rho, rho));
+    CK(h2d(d_gvp, g_vp));
+    CK(h2d(d_grho, g_rho));
+    if (!ac) {
+        CK(h2d(d_vs, vs));
+        CK(h2d(d_gvs, g_vs));
+    }
+    if (lim) {
+        CK(h2d(d_vp0, vp_start));
+        CK(h2d(d_rho0, rho_start));
+        if (!ac) CK(h2d(d_vs0, vs_start));
+    }
+    CK(cudaMemsetAsync(d_mx, 0, 64, c->st));
+    k_mc_maxima<<<(unsigned)std::min<long long>((N + 255) / 256, 148 * 8), 256, 0, c->st>>>(
+        m, d_vp, d_gvp, d_vs, d_gvs, d_rho, d_grho, d_mx);
+    k_mc_update<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(m, d_mx, d_vp, d_vs, d_rho, d_gvp, d_gvs, d_grho,
+                                                                 d_vp0, d_vs0, d_rho0, d_vp1, d_vs1, d_rho1,
+                                                                 m.lbfgs_npar ? d_s : nullptr, d_eps, d_hit);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(vp1, d_vp1, pb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(rho1, d_rho1, pb, cudaMemcpyDeviceToHost, c->st));
+    if (!ac) CK(cudaMemcpyAsync(vs1, d_vs1, pb, cudaMemcpyDeviceToHost, c->st));
+    if (m.itest == 0) {
+        CK(cudaMemcpyAsync(vp, d_vp, pb, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(rho, d_rho, pb, cudaMemcpyDeviceToHost, c->st));
+        if (!ac) CK(cudaMemcpyAsync(vs, d_vs, pb, cudaMemcpyDeviceToHost, c->st));
+        if (m.lbfgs_npar) CK(cudaMemcpyAsync(s_lbfgs, d_s, (size_t)m.lbfgs_npar * pb, cudaMemcpyDeviceToHost, c->st));
+    }
+    float e[3];
+    int hit = 0;
+    CK(cudaMemcpyAsync(e, d_eps, sizeof e, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&hit, d_hit, sizeof hit, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (eps) std::memcpy(eps, e, sizeof e);
+    if (ratio_hit) *ratio_hit = hit;
     return IFOS_OK;
 }
 

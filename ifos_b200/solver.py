@@ -254,6 +254,42 @@ class ShotSolver:
                                                   int(method), float(f_high_pass)))
         return d
 
+    def mat_change_test(self, model, direction, eps_scale, iter, itest=1, start=None, lbfgs=False, **limits):
+        """Test model of a step-length trial (itest != 0), or the model update
+        itself (itest 0), as src/calc_mat_change_test.c computes it on one
+        rank (PARAMETERIZATION 1).  model, direction and start are dicts of
+        NY x NX planes: vp, vs, rho; the search directions are the driver's
+        waveconv (vp), waveconv_u (vs) and waveconv_rho (rho).  `limits`
+        holds the remaining fields of ifos_mat_change (inv_vp_iter,
+        vp_lower, ..., limit_update, s_vp, ...; lbfgs_npar with vs_avg,
+        rho_avg, vp_avg).  Returns (test model dict, eps (3,), ratio_hit,
+        L-BFGS difference vectors or None); with itest 0 the arrays of
+        `model` are updated in place."""
+        from ._lib import IfosMatChange
+        ac = bool(self.p.acoustic)
+        mc = IfosMatChange(eps_scale=float(eps_scale), iter=int(iter), itest=int(itest),
+                           lbfgs_unnormalised=int(bool(lbfgs)))
+        defaults = dict(vp_lower=0.0, vp_upper=1e30, vs_lower=0.0, vs_upper=1e30, rho_lower=0.0, rho_upper=1e30)
+        for k, v in {**defaults, **limits}.items():
+            setattr(mc, k, v)
+        names = ("vp", "rho") if ac else ("vp", "vs", "rho")
+        for k in names:
+            if model[k].dtype != np.float32 or not model[k].flags.c_contiguous:
+                raise ValueError("model planes must be C-contiguous float32 (they are updated in place)")
+        g = {k: _f32(direction[k]) for k in names}
+        st = {k: _f32(start[k]) for k in names} if start is not None else {}
+        out = {k: np.empty_like(model[k]) for k in names}
+        n = self.p.nx * self.p.ny
+        s = np.zeros(3 * n, np.float32) if (itest == 0 and mc.lbfgs_npar) else None
+        eps = np.zeros(3, np.float32)
+        hit = C.c_int(0)
+        P = lambda d, k: _fp(d[k]) if k in d else None
+        self._check(self.lib.ifos_mat_change_test(
+            self._ctx, C.byref(mc), _fp(model["vp"]), P(model, "vs") if not ac else None, _fp(model["rho"]),
+            P(g, "vp"), P(g, "vs"), P(g, "rho"), P(st, "vp"), P(st, "vs"), P(st, "rho"),
+            P(out, "vp"), P(out, "vs"), P(out, "rho"), _fp(s) if s is not None else None, _fp(eps), C.byref(hit)))
+        return out, eps, bool(hit.value), s
+
     def trkill_table(self, rec_xy, src_xy, lower, upper, table=None):
         """Offset-based trace-kill table (src/create_trkill_table.c): rec_xy
         (2, ntr) receiver grid indices, src_xy (2, nsrc) source coordinates in

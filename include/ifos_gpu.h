@@ -288,6 +288,37 @@ int ifos_taper_grad_shot(ifos_ctx *ctx, int nshots, const float *src_xy, float s
  * to 31; bit-identical to the reference's median2d selection. */
 int ifos_median_smooth(ifos_ctx *ctx, float *mat, int filt_size);
 
+/* Test model of a step-length trial, or the model update itself
+ * (src/calc_mat_change_test.c:26-334, PARAMETERIZATION 1, one rank): each
+ * parameter's step is eps_scale * max(model) / max|search direction| (0
+ * before its INV_*_ITER iteration; eps_scale itself under unnormalised
+ * L-BFGS steps), then the reference's bounds, Vp/Vs ratio, limited-update
+ * (S) and sign rules, in its float/double arithmetic.  The search
+ * directions are the driver's waveconv, waveconv_u, waveconv_rho. */
+typedef struct ifos_mat_change {
+    float eps_scale;                       /* eps_scale: the trial's scale */
+    int iter, itest;                       /* iter; itest 0 updates vp/vs/rho in place */
+    int inv_vp_iter, inv_vs_iter, inv_rho_iter;  /* INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER */
+    int lbfgs_unnormalised;                /* GRAD_METHOD==2 && iter > LBFGS_iter_start && LBFGS_STEP_LENGTH */
+    float vp_lower, vp_upper, vs_lower, vs_upper, rho_lower, rho_upper; /* VPLOWERLIM ... RHOUPPERLIM */
+    float vp_vs_ratio;                     /* VP_VS_RATIO (checked when > 1) */
+    int limit_update;                      /* S */
+    float s_vp, s_vs, s_rho;               /* S_VP, S_VS, S_RHO (percent) */
+    int lbfgs_npar;                        /* LBFGS_NPAR of the difference vectors (itest 0), 0: none */
+    float vs_avg, rho_avg, vp_avg;         /* Vs_avg, rho_avg, Vp_avg of the difference vectors */
+} ifos_mat_change;
+/* Host NY x NX planes.  vs, g_vs, vs_start and vs1 are unused (may be NULL)
+ * when the context is acoustic; the *_start planes are read only when
+ * limit_update is set.  vp1, vs1, rho1 receive the test model; with itest 0
+ * vp, vs, rho are also replaced by it and, when s_lbfgs is not NULL, the
+ * difference vectors (vs, rho, vp planes of NX*NY, in the reference's
+ * column-major order) are written there.  eps[3] receives EPSILON,
+ * EPSILON_u, EPSILON_rho; *ratio_hit is set when the Vp/Vs bound moved vp. */
+int ifos_mat_change_test(ifos_ctx *ctx, const ifos_mat_change *mc, float *vp, float *vs, float *rho,
+                         const float *g_vp, const float *g_vs, const float *g_rho, const float *vp_start,
+                         const float *vs_start, const float *rho_start, float *vp1, float *vs1, float *rho1,
+                         float *s_lbfgs, float *eps, int *ratio_hit);
+
 /* Step length of the line search (src/calc_opt_step.c:73-112, solving with
  * src/solvelin.c:53-70): fits the parabola a + b*eps + c*eps^2 through the
  * misfits l2t[0..2] of the test steps epst[0..2] by Gaussian elimination

@@ -3,7 +3,8 @@
  *
  * Link stand-ins for reference entry points that need FFTW3 or SU file input
  * (absent here) and are off the path the oracle exercises (LNORM=2, analytic
- * source wavelets).  Each aborts loudly if ever reached.
+ * source wavelets); those abort loudly if ever reached.  The file writers
+ * and the parameter broadcast below are single-rank no-ops.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -17,6 +18,12 @@ void calc_hilbert(float **a, float **b, int ns, int ntr) { (void)a; (void)b; (vo
 void inseis_source_wavelet(float *a, int nt, int ishot, int sh, int stf) {
     (void)a; (void)nt; (void)ishot; (void)sh; (void)stf; off_path("inseis_source_wavelet");
 }
-/* model file merging of src/mergemod.c (called by the file writers of
- * src/matrix_operations.c, which the smoothing oracle links but never calls) */
-void mergemod(char modfile[74], int format) { (void)modfile; (void)format; off_path("mergemod"); }
+/* model file merging of src/mergemod.c and the per-rank model writer of
+ * src/writemod.c: src/calc_mat_change_test.c writes the updated model and
+ * the L-BFGS difference vectors through them after its arithmetic; the files
+ * are off the oracle's path, so both are no-ops here */
+void mergemod(char modfile[74], int format) { (void)modfile; (void)format; }
+void writemod(char modfile[74], float **array, int format) { (void)modfile; (void)array; (void)format; }
+/* src/exchange_par.c broadcasts the parameters from rank 0; with one rank
+ * that is the identity */
+void exchange_par(void) {}
