@@ -7,8 +7,9 @@ misfits and fits a parabola through the three (step, misfit) pairs
 (src/calc_opt_step.c).  Here every (test model, shot) pair is one slot of a
 single context, so all the test forwards of a search step together in one
 kernel per time step; the misfits come from the FP64 device residual and
-the fit is ``ifos_opt_step``.  Building the test models (the reference's
-calc_mat_change_test with its limits) stays with the caller.
+the fit is ``ifos_opt_step``.  The test models themselves come from
+``trial_models``: the reference's calc_mat_change_test with its limits, on
+the device (``ifos_mat_change_test``).
 """
 from __future__ import annotations
 
@@ -48,6 +49,23 @@ def trial_misfits(p: ShotParams, models: Sequence[Dict[str, np.ndarray]], shots:
             for k, (mi, _) in enumerate(batch):
                 out[mi] += l2[k]
     return out
+
+
+def trial_models(p: ShotParams, model: Dict[str, np.ndarray], direction: Dict[str, np.ndarray],
+                 eps_scales: Sequence[float], iter: int, start=None, device: int = 0, **limits):
+    """The test model of every step scale (src/calc_mat_change_test.c with
+    itest != 0, as src/IFOS2D.c:3285-3330 calls it for each trial) and the
+    step lengths EPSILON / EPSILON_u / EPSILON_rho it used.  `limits` are
+    the remaining fields of ifos_mat_change (INV_*_ITER, bounds, VP_VS_RATIO,
+    S and S_*)."""
+    models, eps = [], []
+    with ShotSolver(p, snapshots=False, device=device) as s:
+        for k, scale in enumerate(eps_scales):
+            m, e, _, _ = s.mat_change_test({k_: np.ascontiguousarray(v, np.float32) for k_, v in model.items()},
+                                           direction, scale, iter, itest=k + 1, start=start, **limits)
+            models.append(m)
+            eps.append(e)
+    return models, np.array(eps, np.float32)
 
 
 def step_length(p: ShotParams, models: Sequence[Dict[str, np.ndarray]], eps: Sequence[float], shots, observed,

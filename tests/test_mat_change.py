@@ -133,3 +133,26 @@ def test_mat_change_test_matches_reference(name):
         assert hit and (got["vp"] != m["vp"]).any()
         clamped = (got["vp"] == 2200.0) | (got["vp"] == 3100.0)
         assert clamped.any()
+
+
+def test_trial_models_of_the_line_search():
+    """linesearch.trial_models builds the three test models of a step-length
+    search (itest 1..3) without touching the current model; each equals the
+    reference's test model of its scale."""
+    from ifos_b200 import linesearch as LS
+    from ifos_b200.params import ShotParams
+    rng = np.random.default_rng(11)
+    m, g = _model(rng, False)
+    kw = dict(inv_vp_iter=0, inv_vs_iter=0, inv_rho_iter=0, vp_lower=2000.0, vp_upper=3300.0, vs_lower=900.0,
+              vs_upper=2000.0, rho_lower=1800.0, rho_upper=2700.0, vp_vs_ratio=0.0, limit_update=0, s_vp=0.0,
+              s_vs=0.0, s_rho=0.0, vs_avg=1.0, vp_avg=1.0, rho_avg=1.0)
+    p = ShotParams(nx=NX, ny=NY, nt=20, dh=1.0, dt=1e-3, fdorder=4, fw=4)
+    before = {k: v.copy() for k, v in m.items()}
+    models, eps = LS.trial_models(p, m, g, [0.01, 0.02, 0.04], iter=2, **kw)
+    assert all(np.array_equal(m[k], before[k]) for k in m)
+    for k_, scale in enumerate([0.01, 0.02, 0.04]):
+        want, _, want_eps, _ = _ref_run({k: v.copy() for k, v in m.items()}, g, m, dict(kw), False, 2, k_ + 1, scale,
+                                        0, False)
+        for k in want:
+            assert np.array_equal(models[k_][k].view(np.int32), want[k].view(np.int32)), (k_, k)
+        assert np.array_equal(eps[k_].view(np.int32), want_eps.view(np.int32))
