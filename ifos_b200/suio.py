@@ -3,7 +3,8 @@
 ``write_su`` writes what src/outseis_glob.c writes for SEIS_FORMAT=1 (SU
 traces without a file header): one 240-byte SEG-Y trace header per trace
 with the fields that routine sets (src/outseis_glob.c:75-268), followed by
-the trace's float32 samples.  ``read_observed`` reads such a file the way
+the trace's float32 samples.  ``save_seismograms`` writes the set of files
+src/saveseis_glob.c writes for one shot.  ``read_observed`` reads such a file the way
 src/inseis.c:71-84 does for the inversion: sample 1 of every trace is set to
 zero and samples 2..ns are kept.  The header layout is the standard SU one
 (src/segy.h): bytes 211-240 (shortpad, unass) are not set by the reference
@@ -114,3 +115,81 @@ def read_observed(path: str, ntr: int, ns: int):
     out = np.array(data[:ntr], np.float32)
     out[:, 0] = 0.0
     return out
+
+
+# the file-name stem of each kind of seismogram src/saveseis_glob.c:43-133
+# writes (type_switch 1-4), "{c}" standing for the component
+_KIND = {1: "{c}.su.syn.shot{s}.it{i}", 2: "{c}.su.shot{s}_adjoint_src", 4: "{c}.su.syn.adj.shot{s}.it{i}"}
+_FILTERED = {1: "{c}.su.obs.shot{s}.it{i}", 2: "{c}.su.obs.adj.shot{s}.it{i}"}
+
+
+def seismogram_files(seis_file: str, ishot: int, iter: int, kind: int, seismo: int, wavetype: int = 1,
+                     adjoint_type: int = 1, forward_only: int = 0, write_filtered_data: int = 0):
+    """The (component, path) pairs src/saveseis_glob.c writes, in its order:
+    kind (type_switch) 1 synthetic, 2 residual (adjoint source), 3 filtered
+    observed (WRITE_FILTERED_DATA 1 or 2), 4 filtered synthetic; FORWARD_ONLY
+    names every file ``<SEIS_FILE>_<c>.su.shot<ishot>``.  Components by
+    SEISMO (src/saveseis_glob.c:152-238): 1 vx/vy (by ADJOINT_TYPE; both when
+    forward only) and vz, 2 p, 3 div and curl, 4 velocities, p, div, curl and
+    vz, 5 velocities, p and vz."""
+    if forward_only == 1:
+        stem = "{c}.su.shot{s}"
+    elif kind == 3:
+        if write_filtered_data not in _FILTERED:
+            raise ValueError("filtered observed data need WRITE_FILTERED_DATA 1 or 2")
+        stem = _FILTERED[write_filtered_data]
+    elif kind in _KIND:
+        stem = _KIND[kind]
+    else:
+        raise ValueError("saveseis_glob: Unkown type_switch")
+    psv, sh = wavetype in (1, 3), wavetype in (2, 3)
+    out = []
+
+    def add(c):
+        out.append((c, f"{seis_file}_" + stem.format(c=c, s=ishot, i=iter)))
+
+    def velocities(both_when_forward):
+        if adjoint_type == 1 or (both_when_forward and forward_only == 1):
+            add("vx")
+            add("vy")
+        if adjoint_type == 2:
+            add("vy")
+        if adjoint_type == 3:
+            add("vx")
+
+    if seismo == 1:
+        if psv:
+            velocities(True)
+        if sh:
+            add("vz")
+    elif seismo == 2:
+        add("p")
+    elif seismo == 3:
+        add("div")
+        add("curl")
+    elif seismo in (4, 5):
+        if psv:
+            velocities(False)
+            add("p")
+            if seismo == 4:
+                add("div")
+                add("curl")
+        if sh:
+            add("vz")
+    return out
+
+
+def save_seismograms(seis_file: str, sections: dict, recpos, src_xy, ishot: int, iter: int, kind: int, seismo: int,
+                     dh: float, dt: float, refrec=(0.0, 0.0), ndt: int = 1, wavetype: int = 1, adjoint_type: int = 1,
+                     forward_only: int = 0, write_filtered_data: int = 0):
+    """Write one shot's seismograms as src/saveseis_glob.c does (SU,
+    SEIS_FORMAT=1): `sections` maps vx, vy, vz, p, div, curl to (ntr, ns)
+    arrays, recpos is (3, ntr) grid x, grid y and global trace number,
+    src_xy the shot's source position in metres.  Returns the paths
+    written."""
+    comp = {"vx": 1, "vy": 2, "vz": 2}
+    files = seismogram_files(seis_file, ishot, iter, kind, seismo, wavetype, adjoint_type, forward_only,
+                             write_filtered_data)
+    for c, path in files:
+        write_su(path, sections[c], recpos, src_xy, dh, dt, refrec, comp=comp.get(c, 0), ndt=ndt)
+    return [path for _, path in files]

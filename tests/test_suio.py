@@ -99,3 +99,54 @@ def test_observed_reader_matches_inseis():
     got = suio.read_observed(f"{stem}_vx.su.shot4", ntr, ns)
     assert np.array_equal(got, want)
     assert (got[:, 0] == 0).all() and np.array_equal(got[:, 1:], sec[:, 1:])
+
+
+@pytest.mark.parametrize("kind,seismo,wavetype,adjoint_type,forward_only,wfd", [
+    (1, 1, 1, 1, 0, 0), (1, 4, 3, 1, 0, 0), (2, 5, 1, 3, 0, 0), (3, 1, 3, 2, 0, 1), (3, 4, 1, 1, 0, 2),
+    (4, 3, 1, 1, 0, 0), (1, 2, 1, 1, 1, 0), (1, 1, 1, 2, 1, 0)])
+def test_seismogram_files_match_saveseis_glob(kind, seismo, wavetype, adjoint_type, forward_only, wfd):
+    """One shot's seismogram files (names, components and bytes) against
+    src/saveseis_glob.c for every kind of data, SEISMO mode and the
+    forward-only naming."""
+    ref, _ = H.libs()
+    rng = np.random.default_rng(kind * 10 + seismo)
+    ntr, ns, dh, dt, ishot, it = 9, 40, 2.0, 5e-4, 2, 3
+    names = ["vx", "vy", "vz", "p", "curl", "div"]
+    secs = {n: rng.standard_normal((ntr, ns)).astype(np.float32) for n in names}
+    rx, ry, rn = rng.integers(3, 200, ntr), rng.integers(1, 30, ntr), np.arange(1, ntr + 1) + 7
+    src = np.array([[10.0, 33.5, 71.0], [4.0, 6.5, 2.0]], np.float32)  # srcpos rows 1-2 of three shots
+    _set(ref, dh, dt, ns, 1, (0.0, 0.0))
+    for name, v in (("SEISMO", seismo), ("SEIS_FORMAT", 1), ("WAVETYPE", wavetype), ("VERBOSE", 0),
+                    ("FORWARD_ONLY", forward_only), ("ADJOINT_TYPE", adjoint_type), ("WRITE_FILTERED_DATA", wfd),
+                    ("RUN_MULTIPLE_SHOTS", 1), ("VELOCITY", 0)):
+        C.c_int.in_dll(ref, name).value = v
+    da, db = tempfile.mkdtemp(prefix="sr"), tempfile.mkdtemp(prefix="so")
+    (C.c_char * 74).in_dll(ref, "SEIS_FILE").value = os.path.join(da, "seis").encode()
+    M = {}
+    for n in names:
+        M[n] = ref.matrix(1, ntr, 1, ns)
+        for t in range(ntr):
+            for j in range(ns):
+                M[n][t + 1][j + 1] = float(secs[n][t, j])
+    R = ref.imatrix(1, 3, 1, ntr)
+    for t in range(ntr):
+        R[1][t + 1], R[2][t + 1], R[3][t + 1] = int(rx[t]), int(ry[t]), int(rn[t])
+    P = ref.matrix(1, 8, 1, 3)
+    for k in range(3):
+        P[1][k + 1], P[2][k + 1] = float(src[0, k]), float(src[1, k])
+    libc = _libc()
+    log = libc.fopen(os.devnull.encode(), b"w")
+    f = ref.saveseis_glob
+    f.restype = None
+    f.argtypes = [C.c_void_p] + [H.FPP] * 6 + [H.IPP, H.IPP, C.c_int, H.FPP, C.c_int, C.c_int, C.c_int, C.c_int]
+    f(log, M["vx"], M["vy"], M["vz"], M["p"], M["curl"], M["div"], R, R, ntr, P, ishot, ns, it, kind)
+    libc.fclose(log)
+    paths = suio.save_seismograms(os.path.join(db, "seis"), secs, np.stack([rx, ry, rn]), src[:, ishot - 1], ishot,
+                                  it, kind, seismo, dh, dt, wavetype=wavetype, adjoint_type=adjoint_type,
+                                  forward_only=forward_only, write_filtered_data=wfd)
+    assert sorted(os.listdir(da)) == sorted({os.path.basename(p) for p in paths}) and paths
+    rec = 240 + 4 * ns
+    for path in set(paths):
+        a = np.fromfile(os.path.join(da, os.path.basename(path)), np.uint8).reshape(ntr, rec)
+        b = np.fromfile(path, np.uint8).reshape(ntr, rec)
+        assert np.array_equal(a[:, :210], b[:, :210]) and np.array_equal(a[:, 240:], b[:, 240:]), path
