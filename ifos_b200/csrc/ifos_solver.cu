@@ -125,6 +125,12 @@ struct ifos_ctx {
     float last_ms = 0.0f;
     long long launches = 0;
     cudaStream_t own_st = nullptr;  // the context's own stream (st may be a caller's)
+    // asynchronous fetches: a copy stream, the event a copy waits for, and
+    // per buffer the completion of its latest copy (pending until a later
+    // writer of the buffer has been ordered after it)
+    cudaStream_t cp_st = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_sec_done = nullptr, ev_grad_done = nullptr;
+    bool sec_pending = false, grad_pending = false;
     // sampled per-kernel timing
     int prof_stride = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -353,6 +359,7 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
     if (!c) return IFOS_OK;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->cp_st) cudaStreamSynchronize(c->cp_st);  // asynchronous fetches still reading the buffers
     DevBuf *bufs[] = {&c->state, &c->psi, &c->models, &c->prof, &c->srf, &c->slot_model, &c->src_pos, &c->src_sig,
                       &c->src_n, &c->rec_pos, &c->rec_n, &c->adj, &c->sec, &c->snap, &c->snap_scale, &c->gacc,
                       &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
@@ -363,6 +370,9 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
     if (c->cap_st) cudaStreamDestroy(c->cap_st);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->cp_st) cudaStreamDestroy(c->cp_st);
+    for (cudaEvent_t e : {c->ev_ready, c->ev_sec_done, c->ev_grad_done})
+        if (e) cudaEventDestroy(e);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     delete c;
     return IFOS_OK;
@@ -1373,10 +1383,26 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     return IFOS_OK;
 }
 
+// Orders the context's stream after the asynchronous fetches still reading
+// the seismogram (sec) or gradient (grads) buffers, before work that
+// overwrites them; the host does not wait.
+static int order_after_fetches(ifos_ctx *c, bool sec, bool grads) {
+    if (sec && c->sec_pending) {
+        CK(cudaStreamWaitEvent(c->st, c->ev_sec_done, 0));
+        c->sec_pending = false;
+    }
+    if (grads && c->grad_pending) {
+        CK(cudaStreamWaitEvent(c->st, c->ev_grad_done, 0));
+        c->grad_pending = false;
+    }
+    return IFOS_OK;
+}
+
 extern "C" int ifos_forward(ifos_ctx *c, int nshots, int store, float *sections) {
     if (!c) return IFOS_ERR_ARG;
     if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    if (int rc = order_after_fetches(c, true, false)) return rc;
     int rc = c->dbl ? forward_t<double>(c, nshots, store, c->p.nt) : forward_t<float>(c, nshots, store, c->p.nt);
     if (rc == IFOS_OK && sections) rc = ifos_fetch_sections(c, nshots, sections);
     return rc;
@@ -1404,6 +1430,7 @@ extern "C" int ifos_adjoint(ifos_ctx *c, int nshots, const float *adj, float *gr
         return fail(c, IFOS_ERR_STATE, "no adjoint sources staged");
     }
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, IFOS_ERR_CUDA, "cudaSetDevice failed");
+    if (int rc = order_after_fetches(c, false, true)) return rc;
     int rc = c->dbl ? adjoint_t<double>(c, nshots) : adjoint_t<float>(c, nshots);
     if (rc == IFOS_OK && grads) rc = ifos_fetch_grads(c, nshots, grads);
     return rc;
@@ -1426,6 +1453,73 @@ extern "C" int ifos_fetch_grads(ifos_ctx *c, int nshots, float *grads) {
     CK(cudaMemcpyAsync(grads, c->gout.p, (size_t)nshots * IFOS_NG * c->p.nx * c->p.ny * 4, cudaMemcpyDeviceToHost,
                        c->st));
     CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+// An asynchronous device-to-host copy on the context's copy stream, after the
+// work already on its stream; *done marks its completion.
+static int fetch_async(ifos_ctx *c, void *dst, const void *src, size_t bytes, cudaEvent_t done, bool *pending) {
+    CK(cudaEventRecord(c->ev_ready, c->st));
+    CK(cudaStreamWaitEvent(c->cp_st, c->ev_ready, 0));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->cp_st));
+    CK(cudaEventRecord(done, c->cp_st));
+    *pending = true;
+    return IFOS_OK;
+}
+
+static int copy_stream(ifos_ctx *c) {
+    if (c->cp_st) return IFOS_OK;
+    CK(cudaStreamCreateWithFlags(&c->cp_st, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&c->ev_ready, &c->ev_sec_done, &c->ev_grad_done})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_fetch_sections_async(ifos_ctx *c, int nshots, float *sections) {
+    if (!c || !sections) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    if (int rc = copy_stream(c)) return rc;
+    return fetch_async(c, sections, c->sec.p, (size_t)nshots * IFOS_NS * std::max(1, c->p.max_rec) * c->p.nt * 4,
+                       c->ev_sec_done, &c->sec_pending);
+}
+
+extern "C" int ifos_fetch_grads_async(ifos_ctx *c, int nshots, float *grads) {
+    if (!c || !grads) return IFOS_ERR_ARG;
+    if (nshots < 1 || nshots > c->p.max_shots) return fail(c, IFOS_ERR_ARG, "nshots out of range");
+    CK(cudaSetDevice(c->device));
+    if (int rc = copy_stream(c)) return rc;
+    return fetch_async(c, grads, c->gout.p, (size_t)nshots * IFOS_NG * c->p.nx * c->p.ny * 4, c->ev_grad_done,
+                       &c->grad_pending);
+}
+
+extern "C" int ifos_fetch_wait(ifos_ctx *c) {
+    if (!c) return IFOS_ERR_ARG;
+    if (!c->cp_st) return IFOS_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->cp_st));
+    c->sec_pending = c->grad_pending = false;
+    return IFOS_OK;
+}
+
+extern "C" int ifos_host_alloc(size_t bytes, void **out) {
+    if (!out) return IFOS_ERR_ARG;
+    *out = nullptr;
+    const cudaError_t e = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        ifos_internal_set_error(std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+        return IFOS_ERR_NOMEM;
+    }
+    return IFOS_OK;
+}
+
+extern "C" int ifos_host_free(void *p) {
+    if (!p) return IFOS_OK;
+    const cudaError_t e = cudaFreeHost(p);
+    if (e != cudaSuccess) {
+        ifos_internal_set_error(std::string("cudaFreeHost: ") + cudaGetErrorString(e));
+        return IFOS_ERR_CUDA;
+    }
     return IFOS_OK;
 }
 
@@ -1508,6 +1602,7 @@ extern "C" int ifos_forward_steps(ifos_ctx *c, int nsteps, float *fields) {
     if (!c) return IFOS_ERR_ARG;
     if (nsteps < 1 || nsteps > c->p.nt) return fail(c, IFOS_ERR_ARG, "nsteps out of range");
     CK(cudaSetDevice(c->device));
+    if (int rc = order_after_fetches(c, true, false)) return rc;
     int rc = c->dbl ? forward_t<double>(c, 1, 0, nsteps) : forward_t<float>(c, 1, 0, nsteps);
     if (rc == IFOS_OK && fields) rc = ifos_fetch_fields(c, 0, fields);
     return rc;
@@ -1815,6 +1910,7 @@ extern "C" int ifos_taper_grad_shot(ifos_ctx *c, int nshots, const float *src_xy
     if (!c || !src_xy || nshots < 1 || nshots > c->p.max_shots) return IFOS_ERR_ARG;
     if (srtshape != 1 && srtshape != 2) return fail(c, IFOS_ERR_ARG, "SRTSHAPE must be 1 or 2");
     CK(cudaSetDevice(c->device));
+    if (int rc = order_after_fetches(c, false, true)) return rc;
     const ifos_params &p = c->p;
     const float dh = p.dh;
     int gp = 0;

@@ -59,6 +59,36 @@ def opt_step(l2t, epst, fp64: bool = True) -> float:
     return out.value
 
 
+class PinnedBuffer:
+    """Page-locked host memory (``ifos_host_alloc``) as a numpy array, the
+    destination that lets an asynchronous fetch overlap the device work that
+    follows it.  Freed by ``close()`` or when the buffer is collected; the
+    array must not be used after that."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.lib = _lib.load()
+        dt = np.dtype(dtype)
+        n = int(np.prod(shape)) * dt.itemsize
+        self._ptr = C.c_void_p()
+        rc = self.lib.ifos_host_alloc(n, C.byref(self._ptr))
+        if rc != 0:
+            raise IfosError(rc, self.lib.ifos_last_error(None).decode())
+        raw = (C.c_char * max(n, 1)).from_address(self._ptr.value)
+        self.array = np.frombuffer(raw, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+    def close(self):
+        if self._ptr:
+            self.array = None
+            self.lib.ifos_host_free(self._ptr)
+            self._ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ShotSolver:
     """One device context: ``max_shots`` shot slots stepped together."""
 
@@ -71,6 +101,7 @@ class ShotSolver:
                                   hi_order_corrected=hi_order_corrected)
         self.max_shots, self.max_rec, self.max_src = int(max_shots), int(max_rec), int(max_src)
         self._ctx = C.c_void_p()
+        self._inflight = []  # host arrays of asynchronous fetches not yet waited for
         rc = self.lib.ifos_ctx_create(C.byref(self.params), int(device), 1 if snapshots else 0, C.byref(self._ctx))
         if rc != 0:
             raise IfosError(rc, self.lib.ifos_last_error(None).decode())
@@ -86,8 +117,9 @@ class ShotSolver:
 
     def close(self):
         if self._ctx:
-            self.lib.ifos_ctx_destroy(self._ctx)
+            self.lib.ifos_ctx_destroy(self._ctx)  # waits for asynchronous fetches
             self._ctx = C.c_void_p()
+            self._inflight = []
 
     def __enter__(self):
         return self
@@ -149,6 +181,33 @@ class ShotSolver:
         out = np.zeros((nshots, NG, self.p.ny, self.p.nx), np.float32)
         self._check(self.lib.ifos_fetch_grads(self._ctx, int(nshots), _fp(out)))
         return out
+
+    def fetch_sections_async(self, nshots, out):
+        """Queue the copy of the seismograms of slots [0, nshots) into `out`
+        ((nshots, 6, max_rec, NT) float32, best a ``PinnedBuffer`` array) and
+        return at once; `out` is complete after ``fetch_wait``."""
+        self._check_out(out, (nshots, NS, self.max_rec, self.p.nt))
+        self._check(self.lib.ifos_fetch_sections_async(self._ctx, int(nshots), _fp(out)))
+        self._inflight.append(out)
+        return out
+
+    def fetch_grads_async(self, nshots, out):
+        """Queue the copy of the per-shot gradients of slots [0, nshots) into
+        `out` ((nshots, 10, NY, NX) float32); complete after ``fetch_wait``."""
+        self._check_out(out, (nshots, NG, self.p.ny, self.p.nx))
+        self._check(self.lib.ifos_fetch_grads_async(self._ctx, int(nshots), _fp(out)))
+        self._inflight.append(out)
+        return out
+
+    def fetch_wait(self):
+        """Block until every queued asynchronous fetch has landed."""
+        self._check(self.lib.ifos_fetch_wait(self._ctx))
+        self._inflight.clear()
+
+    @staticmethod
+    def _check_out(out, shape):
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.shape != tuple(shape):
+            raise ValueError(f"output must be a C-contiguous float32 array of shape {tuple(shape)}")
 
     def grad_sum(self, nshots=1):
         out = np.zeros((5, self.p.ny, self.p.nx), np.float32)

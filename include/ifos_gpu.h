@@ -148,6 +148,22 @@ int ifos_adjoint(ifos_ctx *ctx, int nshots, const float *adj, float *grads);
 int ifos_stage_adjoint(ifos_ctx *ctx, int nshots, const float *adj);
 int ifos_fetch_sections(ifos_ctx *ctx, int nshots, float *sections);
 int ifos_fetch_grads(ifos_ctx *ctx, int nshots, float *grads);
+/* Asynchronous device-to-host staging of the same buffers (the driver's
+ * seismogram and gradient output, src/saveseis_glob.c and the gradient
+ * writers, without the host waiting on the device): the copy is queued on
+ * the context's copy stream after the work already queued and the call
+ * returns at once, so it overlaps the next forward or adjoint.  A later call
+ * that overwrites the buffer (ifos_forward / ifos_forward_steps for the
+ * seismograms, ifos_adjoint / ifos_taper_grad_shot for the gradients) is
+ * ordered after the copy on the device.  The host memory must stay valid,
+ * and is not to be read, until ifos_fetch_wait returns; it overlaps only
+ * when pinned (ifos_host_alloc). */
+int ifos_fetch_sections_async(ifos_ctx *ctx, int nshots, float *sections);
+int ifos_fetch_grads_async(ifos_ctx *ctx, int nshots, float *grads);
+int ifos_fetch_wait(ifos_ctx *ctx);
+/* Pinned (page-locked) host memory for asynchronous fetches; no context. */
+int ifos_host_alloc(size_t bytes, void **out);
+int ifos_host_free(void *p);
 /* Sum of the assembled per-shot gradients (vp, vs, rho, vs_z, rho_z) over
  * slots [0, nshots), as src/IFOS2D.c:2703-2724: out is 5 x NY x NX. */
 int ifos_grad_sum(ifos_ctx *ctx, int nshots, float *out);
