@@ -618,20 +618,29 @@ def main():
     # ---- end to end through the public API with host buffers ----
     e2e = None
     if not args.no_e2e:
-        obs_host = (np.random.default_rng(200 + rank).standard_normal((B, 3, ntr, p.nt)) * 1e-9).astype(np.float32)
+        from ifos_b200.solver import PinnedBuffer
+        # pinned host buffers: observed data in, seismograms and gradients out
+        obs_pin = PinnedBuffer((B, 3, ntr, p.nt))
+        obs_pin.array[...] = np.random.default_rng(200 + rank).standard_normal((B, 3, ntr, p.nt)) * 1e-9
+        sec_pin = PinnedBuffer((B, 6, ntr, p.nt))
+        grad_pin = PinnedBuffer((B, 10, p.ny, p.nx))
+        sec, grads = sec_pin.array, grad_pin.array
         e2e_times = []
         h2d = 0
         for k in range(args.steps):
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
-            h2d = obs_host.nbytes
+            h2d = obs_pin.array.nbytes
             for b in range(B):
                 g, sig = shot((args.warmup + args.steps + k) * B + b)
                 solver.setup_shot(b, g.srcpos, sig, g.recpos)
                 h2d += g.srcpos.nbytes + sig.nbytes + g.recpos.nbytes
-            sec = solver.forward(B, store=True, fetch=True)
-            l2, _ = solver.residual_adjoint(obs_host, B)
-            grads = solver.adjoint(None, B, fetch=True)
+            solver.forward(B, store=True, fetch=False)
+            solver.fetch_sections_async(B, sec)  # overlaps the residual and the adjoint
+            l2, _ = solver.residual_adjoint(obs_pin.array, B)
+            solver.adjoint(None, B, fetch=False)
+            solver.fetch_grads_async(B, grads)
+            solver.fetch_wait()  # this step's seismograms and gradients are on the host
             torch.cuda.synchronize(device)
             e2e_times.append(time.perf_counter() - t0)
         tot = sum(e2e_times)
@@ -641,7 +650,10 @@ def main():
             tot = float(t.item())
         e2e = {"value": total_shots / tot, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(sec.nbytes + grads.nbytes + l2.nbytes),
-               "path": "ShotSolver.setup_shot / forward(fetch) / residual_adjoint(observed) / adjoint(fetch)"}
+               "path": "ShotSolver.setup_shot / forward / fetch_sections_async / residual_adjoint(observed) / "
+                       "adjoint / fetch_grads_async / fetch_wait, pinned host buffers"}
+        for b in (obs_pin, sec_pin, grad_pin):
+            b.close()
     solver.close()
 
     if rank != 0:
