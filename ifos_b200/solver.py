@@ -59,34 +59,47 @@ def opt_step(l2t, epst, fp64: bool = True) -> float:
     return out.value
 
 
-class PinnedBuffer:
-    """Page-locked host memory (``ifos_host_alloc``) as a numpy array, the
-    destination that lets an asynchronous fetch overlap the device work that
-    follows it.  Freed by ``close()`` or when the buffer is collected; the
-    array must not be used after that."""
+class _PinnedMemory:
+    """Owns one ``ifos_host_alloc`` block; frees it once, on ``free()`` or
+    when the last reference (the array's backing buffer) goes."""
 
-    def __init__(self, shape, dtype=np.float32):
-        self.lib = _lib.load()
-        dt = np.dtype(dtype)
-        n = int(np.prod(shape)) * dt.itemsize
-        self._ptr = C.c_void_p()
-        rc = self.lib.ifos_host_alloc(n, C.byref(self._ptr))
+    def __init__(self, lib, nbytes):
+        self.lib = lib
+        self.ptr = C.c_void_p()
+        rc = lib.ifos_host_alloc(nbytes, C.byref(self.ptr))
         if rc != 0:
-            raise IfosError(rc, self.lib.ifos_last_error(None).decode())
-        raw = (C.c_char * max(n, 1)).from_address(self._ptr.value)
-        self.array = np.frombuffer(raw, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+            raise IfosError(rc, lib.ifos_last_error(None).decode())
 
-    def close(self):
-        if self._ptr:
-            self.array = None
-            self.lib.ifos_host_free(self._ptr)
-            self._ptr = C.c_void_p()
+    def free(self):
+        if self.ptr:
+            self.lib.ifos_host_free(self.ptr)
+            self.ptr = C.c_void_p()
 
     def __del__(self):
         try:
-            self.close()
+            self.free()
         except Exception:
             pass
+
+
+class PinnedBuffer:
+    """Page-locked host memory (``ifos_host_alloc``) as a numpy array, the
+    destination that lets an asynchronous fetch overlap the device work that
+    follows it.  Freed when neither the buffer nor its array is referenced
+    any more, or by ``close()``, after which the array must not be used (and
+    which must not come before ``fetch_wait`` of a fetch into it)."""
+
+    def __init__(self, shape, dtype=np.float32):
+        dt = np.dtype(dtype)
+        count = int(np.prod(shape))
+        self._mem = _PinnedMemory(_lib.load(), count * dt.itemsize)
+        raw = (C.c_char * max(count * dt.itemsize, 1)).from_address(self._mem.ptr.value)
+        raw._owner = self._mem  # the array keeps the memory alive (e.g. while an asynchronous fetch writes it)
+        self.array = np.frombuffer(raw, dtype=dt, count=count).reshape(shape)
+
+    def close(self):
+        self.array = None
+        self._mem.free()
 
 
 class ShotSolver:

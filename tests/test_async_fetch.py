@@ -10,7 +10,6 @@ from ifos_b200.solver import PinnedBuffer, ShotSolver
 from tests.golden.cases import build_case
 from tests.gpu_helpers import bit_equal
 
-pytestmark = pytest.mark.gpu
 
 
 def _inputs():
@@ -33,6 +32,7 @@ def _sync_runs(p, model, g, sigs, adjs):
     return out
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("pinned", [True, False])
 def test_async_fetches_survive_the_next_loop(pinned):
     p, model, g, sigs, adjs = _inputs()
@@ -65,3 +65,41 @@ def test_async_fetches_survive_the_next_loop(pinned):
         assert bit_equal(sec_a, want[1][0])
         for b in bufs:
             b.close()
+
+
+def test_pinned_memory_lives_as_long_as_its_array(monkeypatch):
+    """A PinnedBuffer's memory stays allocated while its array is referenced
+    (an asynchronous fetch may still be writing it), is freed once when both
+    are gone or on close(), and never twice (fake allocator, no GPU)."""
+    import ctypes as C
+    import gc
+
+    from ifos_b200 import solver as S
+    freed, keep = [], []
+
+    class FakeLib:
+        def ifos_host_alloc(self, n, ptr):
+            buf = C.create_string_buffer(n)
+            keep.append(buf)
+            ptr._obj.value = C.addressof(buf)
+            return 0
+
+        def ifos_host_free(self, p):
+            freed.append(p.value)
+            return 0
+
+    monkeypatch.setattr(S._lib, "load", lambda: FakeLib())
+    b = S.PinnedBuffer((4, 3))
+    a = b.array
+    a[...] = 2.0
+    del b
+    gc.collect()
+    assert freed == [] and float(a.sum()) == 24.0
+    del a
+    gc.collect()
+    assert len(freed) == 1
+    b = S.PinnedBuffer((2,))
+    b.close()
+    del b
+    gc.collect()
+    assert len(freed) == 2
