@@ -27,7 +27,7 @@ EXPORTS = [
     "ifos_sync", "ifos_trkill_table", "ifos_time_window", "ifos_set_option", "ifos_get_option",
     "ifos_residual_adjoint", "ifos_fetch_snapshot", "ifos_opt_step", "ifos_timedomain_filt",
     "ifos_taper_grad_shot", "ifos_median_smooth", "ifos_mat_change_test", "ifos_fetch_sections_async",
-    "ifos_fetch_grads_async", "ifos_fetch_wait", "ifos_host_alloc", "ifos_host_free",
+    "ifos_fetch_grads_async", "ifos_fetch_wait", "ifos_host_alloc", "ifos_host_free", "ifos_status",
 ]
 OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3}
 
@@ -130,6 +130,7 @@ def load():
         "ifos_fetch_sections_async": (C.c_int, [vp, C.c_int, FP]),
         "ifos_fetch_grads_async": (C.c_int, [vp, C.c_int, FP]),
         "ifos_fetch_wait": (C.c_int, [vp]),
+        "ifos_status": (C.c_int, [vp]),
         "ifos_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
         "ifos_host_free": (C.c_int, [C.c_void_p]),
         "ifos_mat_change_test": (C.c_int, [vp, C.POINTER(IfosMatChange), FP, FP, FP, FP, FP, FP, FP, FP, FP, FP, FP,

@@ -100,6 +100,7 @@ struct ifos_ctx {
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
+    int last_code = 0;  // code of the last failed call, read and cleared by ifos_status
     KGrid g{};
     int psv = 0, sh = 0, ac = 0;
     // state
@@ -202,8 +203,12 @@ static void drop_graph(LoopGraph &lg) {
 
 // ----------------------------------------------------------------------------
 static int fail(ifos_ctx *c, int code, const std::string &msg) {
-    if (c) c->err = msg;
-    else g_create_error = msg;
+    if (c) {
+        c->err = msg;
+        c->last_code = code;
+    } else {
+        g_create_error = msg;
+    }
     return code;
 }
 #define CK(call)                                                                                            \
@@ -1754,6 +1759,22 @@ extern "C" int ifos_residual_adjoint(ifos_ctx *c, int nshots, const float *obs, 
 
 extern "C" double ifos_last_ms(const ifos_ctx *c) { return c ? c->last_ms : 0.0; }
 extern "C" long long ifos_launch_count(const ifos_ctx *c) { return c ? c->launches : 0; }
+extern "C" int ifos_status(ifos_ctx *c) {
+    if (!c) return IFOS_ERR_ARG;
+    int code = c->last_code;
+    c->last_code = IFOS_OK;
+    if (cudaSetDevice(c->device) != cudaSuccess) return IFOS_ERR_CUDA;
+    for (cudaStream_t s : {c->st, c->cp_st}) {
+        if (!s) continue;
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e != cudaSuccess && e != cudaErrorNotReady) {
+            c->err = std::string("stream failed: ") + cudaGetErrorString(e);
+            code = IFOS_ERR_CUDA;
+        }
+    }
+    return code;
+}
+
 extern "C" int ifos_sync(ifos_ctx *c) {
     if (!c) return IFOS_ERR_ARG;
     CK(cudaSetDevice(c->device));

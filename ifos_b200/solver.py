@@ -195,6 +195,11 @@ class ShotSolver:
         self._check(self.lib.ifos_fetch_grads(self._ctx, int(nshots), _fp(out)))
         return out
 
+    def status(self) -> int:
+        """Code of the last failed call since the previous ``status()`` (0:
+        none), or the CUDA error code when the context's streams failed."""
+        return int(self.lib.ifos_status(self._ctx))
+
     def fetch_sections_async(self, nshots, out):
         """Queue the copy of the seismograms of slots [0, nshots) into `out`
         ((nshots, 6, max_rec, NT) float32, best a ``PinnedBuffer`` array) and

@@ -119,6 +119,12 @@ int ifos_ctx_create(const ifos_params *p, int device, int with_snapshots, ifos_c
 int ifos_ctx_destroy(ifos_ctx *ctx);
 /* Last error message of this context (or of the last failed create when ctx is NULL). */
 const char *ifos_last_error(const ifos_ctx *ctx);
+/* Status of a context for a driver that checks once per shot or iteration:
+ * the code of the last failed call since the previous ifos_status (IFOS_OK
+ * when none), or IFOS_ERR_CUDA when its stream or copy stream has failed;
+ * clears the recorded code.  The message stays in ifos_last_error.  The
+ * reference aborts instead (declare_error, src/util.c:26-35). */
+int ifos_status(ifos_ctx *ctx);
 /* Bytes of device memory a context with these parameters needs. */
 size_t ifos_ctx_bytes(const ifos_params *p, int with_snapshots);
 

@@ -223,6 +223,7 @@ def test_error_paths_return_status_not_fault():
         with pytest.raises(IfosError) as e:
             s.setup_shot(0, g.srcpos, sig, bad)
         assert e.value.code == 1
+        assert s.status() == 1 and s.status() == 0  # the last failure, then cleared
     # an unstable model (vp far above the CFL limit) is reported, not hidden
     hot = {k: v.copy() for k, v in model.items()}
     hot["vp"] *= 40.0
