@@ -31,6 +31,7 @@ code (compiled in place) on a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import multiprocessing as mp
@@ -357,18 +358,27 @@ def plain_path(p, models, shots, device, count=2, warmup=1):
             "form": "1 shot per context, fp32 snapshots, step-by-step launches"}
 
 
-def batched_form(device, snap, max_batch=128):
+def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
     """The batched form on its workload: 256 shots round-robin over the
-    plain-elastic start model (400 x 160, FDORDER 4, NT 2000) and 4 seeded
-    perturbations of it, stepped B at a time in one context (B and the
-    execution options from the autotuner, memory permitting), low-precision
-    snapshots, CUDA-graph time loops; against the plain FP32 path on the same
-    shots."""
+    plain-elastic start model (400 x 160, NT 2000) and 4 seeded perturbations
+    of it, stepped B at a time in one context (B and the execution options
+    from the autotuner, memory permitting), low-precision snapshots,
+    CUDA-graph time loops; against the plain FP32 path on the same shots.
+    FDORDER 4 P-SV is the workload as specified; FDORDER 8 (P-SV) and 12 (SH,
+    whose CPML covers every order) repeat it with DT at 0.9 of that order's
+    stability limit."""
     import torch
+    from ifos_b200 import _lib
     from ifos_b200 import autotune as A
     from ifos_b200 import workloads as W
-    from ifos_b200.solver import ShotSolver
+    from ifos_b200.solver import ShotSolver, make_params
     p, true, models, shots = W.batched_perturbed(0, nshots=256)
+    if (fdorder, wavetype) != (p.fdorder, p.wavetype):
+        p.fdorder, p.wavetype = fdorder, wavetype
+        hc = (ctypes.c_float * 7)()
+        _lib.load().ifos_fd_coeffs(ctypes.byref(make_params(p)), hc)
+        vmax = max(float(m["vp"].max()) for m in models)
+        p.dt = W.cfl_dt(p.dh, vmax, sum(abs(hc[m]) for m in range(1, fdorder // 2 + 1)))
     ntr = max(g.recpos.shape[1] for _, g in shots)
     plain = plain_path(p, models, shots, device, count=4)
     free = torch.cuda.mem_get_info(device)[0]
@@ -403,7 +413,8 @@ def batched_form(device, snap, max_batch=128):
         ms = _timed_shots(s, stream, len(shots), run)
         s.set_stream(None)
     value = len(shots) / (ms / 1e3)
-    return {"workload": "batched plain-elastic 400x160 FDORDER4 NT2000 DTINV2, 256 shots over 5 models",
+    physics = "plain-elastic" if wavetype == 1 else "SH elastic"
+    return {"workload": f"batched {physics} 400x160 FDORDER{fdorder} NT2000 DTINV2, 256 shots over 5 models",
             "value": value, "unit": METRIC, "batch": B, "snapshots": snap, "options": choice["options"],
             "ms_all_shots": ms, "plain_fp32": plain, "speedup_vs_plain_fp32": value / plain["value"]}
 
@@ -688,6 +699,10 @@ def main():
             extra["fp64_error"] = {"error": repr(exc)}
     if world == 1:
         for name, flag, fn in (("batched_form", args.no_batched, lambda: batched_form(device, args.snap)),
+                               ("batched_form_fdorder8", args.no_batched,
+                                lambda: batched_form(device, args.snap, fdorder=8)),
+                               ("batched_form_fdorder12_sh", args.no_batched,
+                                lambda: batched_form(device, args.snap, fdorder=12, wavetype=2)),
                                ("serving", args.no_serving,
                                 lambda: serving_bench(device, args.snap, full=args.serving_full)),
                                ("precision", args.no_error, lambda: precision_study(device))):
