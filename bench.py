@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--snap", default="fp16s", choices=["fp32", "bf16", "fp16", "fp16s"],
+    ap.add_argument("--snap", default="fp16s", choices=["fp32", "bf16", "fp16", "fp16s", "i16s"],
                     help="snapshot format of the batched form (the plain FP32 path always stores fp32)")
     ap.add_argument("--batch", type=int, default=0, help="shots per context (0: chosen by the autotuner)")
     ap.add_argument("--max-batch", type=int, default=8)
@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-full", action="store_true", help="full-size serving stream (grids to 3000x1000)")
+    ap.add_argument("--precision-nt", type=int, default=1200,
+                    help="NT of the precision study (8000 is the precision workload's full NT)")
     return ap.parse_args()
 
 
@@ -257,7 +259,8 @@ def fp64_error(p, model, g, nt=300):
     adj = (rng.standard_normal((1, 3, ntr, nt)) * 1e-6).astype(np.float32)
     out = {}
     for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
-                    ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s"))):
+                    ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s")),
+                    ("i16s", dict(snap_format="i16s"))):
         with ShotSolver(q, max_rec=ntr, **kw) as s:
             s.upload_model(model)
             s.setup_shot(0, g.srcpos, sig, g.recpos)
@@ -266,7 +269,7 @@ def fp64_error(p, model, g, nt=300):
         out[tag] = (sec.astype(np.float64), gr.astype(np.float64))
     ref_s, ref_g = out["fp64"]
     res = {"run": f"workload grid, NT={nt}, against fp64 arithmetic with fp64 snapshots"}
-    for tag in ("fp32", "bf16", "fp16", "fp16s"):
+    for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s"):
         s_, g_ = out[tag]
         res[tag] = {"seismogram_rel_l2": _rel(s_[:2], ref_s[:2]), "gradient_rel_l2": _rel(g_[3:6], ref_g[3:6]),
                     "misfit_rel": abs(float(np.sum(s_[:2] ** 2)) - float(np.sum(ref_s[:2] ** 2))) /
@@ -280,8 +283,9 @@ def precision_study(device, nt=1200):
     fp32, bf16, fp16 and fp16-segment snapshots against an fp64 run (fp64
     arithmetic and snapshots) of the same kernels.  The misfit is the FP64
     device misfit of the residual against seeded observed data; the gradient
-    is driven by that residual.  NT is truncated so that the fp64 run's
-    snapshots fit one GPU."""
+    is driven by that residual.  The default NT keeps the default run short;
+    the workload's full NT 8000 fits one GPU at DTINV 20 (77 GB of fp64
+    snapshots)."""
     from ifos_b200 import workloads as W
     from ifos_b200.solver import ShotSolver
     out = {"run": f"4000x1200 precision grid, NT={nt}, DTINV 20, one mid-line shot per wave type"}
@@ -294,7 +298,8 @@ def precision_study(device, nt=1200):
         obs = (rng.standard_normal((1, 3, ntr, p.nt)) * 1e-9).astype(np.float32)
         runs = {}
         for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
-                        ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s"))):
+                        ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s")),
+                    ("i16s", dict(snap_format="i16s"))):
             with ShotSolver(p, max_rec=ntr, device=device, **kw) as s:
                 s.upload_model(model)
                 s.setup_shot(0, g.srcpos, sig, g.recpos)
@@ -305,7 +310,7 @@ def precision_study(device, nt=1200):
         rs, rg, rm = runs["fp64"]
         out[name] = {tag: {"seismogram_rel_l2": _rel(runs[tag][0], rs), "gradient_rel_l2": _rel(runs[tag][1], rg),
                            "misfit_rel": abs(runs[tag][2] - rm) / max(abs(rm), 1e-300)}
-                     for tag in ("fp32", "bf16", "fp16", "fp16s")}
+                     for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s")}
     return out
 
 
@@ -705,7 +710,7 @@ def main():
                                 lambda: batched_form(device, args.snap, fdorder=12, wavetype=2)),
                                ("serving", args.no_serving,
                                 lambda: serving_bench(device, args.snap, full=args.serving_full)),
-                               ("precision", args.no_error, lambda: precision_study(device))):
+                               ("precision", args.no_error, lambda: precision_study(device, nt=args.precision_nt))):
             if flag:
                 continue
             try:

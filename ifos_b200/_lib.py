@@ -15,7 +15,7 @@ MAX_L = 8
 NS, NG, NF = 6, 10, 12
 
 IFOS_OK, IFOS_ERR_ARG, IFOS_ERR_CUDA, IFOS_ERR_NOMEM, IFOS_ERR_UNSTABLE, IFOS_ERR_STATE = range(6)
-SNAP_FORMATS = {"fp32": 0, "bf16": 1, "fp16": 2, "fp16s": 3}
+SNAP_FORMATS = {"fp32": 0, "bf16": 1, "fp16": 2, "fp16s": 3, "i16s": 4}
 
 # every symbol include/ifos_gpu.h declares
 EXPORTS = [

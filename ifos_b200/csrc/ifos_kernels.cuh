@@ -581,6 +581,12 @@ __global__ void k_p_visc(KGrid g, KState<T> S, KModel<T> M) {
 // is stored as zeros.
 constexpr int kSegCells = 64;
 constexpr float kSegTop = 65472.0f;  // 2^15 (2 - 2^-9)
+// int16 segments (IFOS_SNAP_I16S): the same segments and scales, the maximum
+// mapped to 32767 and each value stored as the nearest integer of
+// v * (32767 / m): an absolute error of at most about m / 65534, 32 times
+// below fp16's m / 2048 at the top of the segment (fp16 keeps more relative
+// precision only for values below m / 32).
+constexpr float kSegTopI16 = 32767.0f;
 // all 32 lanes of a warp, each with a column pair of one segment: its maximum |v|
 __device__ __forceinline__ float seg_absmax_warp(float v0, float v1, bool ok0, bool ok1) {
     const unsigned a0 = ok0 ? (__float_as_uint(v0) & 0x7fffffffu) : 0u;
@@ -592,14 +598,25 @@ __device__ __forceinline__ float seg_absmax_warp(float v0, float v1, bool ok0, b
 // ulps of fp32 (far below fp16's 2^-11) and m * q stays below 65504, so the
 // fast approximate division (a reciprocal and a multiply) serves; it is exact
 // enough for m below 2^126 (a wavefield amplitude of 8.5e37).
-__device__ __forceinline__ void seg_scales(float m, float &q, float &inv) {
+__device__ __forceinline__ void seg_scales(float m, float &q, float &inv, float top = kSegTop) {
     if (m >= 1e-30f) {
-        q = __fdividef(kSegTop, m);
-        inv = m * (1.0f / kSegTop);
+        q = __fdividef(top, m);
+        inv = m * (1.0f / top);
     } else {
         q = 0.0f;
         inv = 0.0f;
     }
+}
+
+// the 16-bit pattern of a scaled value x (|x| <= top) and back: fp16 rounded
+// to nearest even, or the nearest integer (clamped to +-32767 against the
+// approximate scale)
+__device__ __forceinline__ unsigned short seg_pack(float x, bool i16) {
+    if (i16) return (unsigned short)(short)__float2int_rn(fminf(fmaxf(x, -kSegTopI16), kSegTopI16));
+    return __half_as_ushort(__float2half_rn(x));
+}
+__device__ __forceinline__ float seg_unpack(unsigned short u, bool i16) {
+    return i16 ? (float)(short)u : __half2float(__ushort_as_half(u));
 }
 
 struct KSnapPatch {

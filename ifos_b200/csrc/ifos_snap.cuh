@@ -27,10 +27,10 @@ template <typename T>
 __device__ inline T snap_load(const KSnap &s, int slot, int snap, int k, long long q) {
     const char *b = (const char *)s.base + slot * s.slot_bytes + snap * s.snap_bytes;
     if (s.format == 0) return ((const T *)b)[k * s.n + q];
-    if (s.format == 3) {
+    if (s.format == 3 || s.format == 4) {
         const long long row = q / s.nx, col = q - row * s.nx;
         const float sc = ((const float *)(b + s.ex_off))[((long long)k * s.ny + row) * s.segs + col / kSegCells];
-        return (T)(__half2float(((const __half *)b)[k * s.n + q]) * sc);
+        return (T)(seg_unpack(((const unsigned short *)b)[k * s.n + q], s.format == 4) * sc);
     }
     const float sc = s.scale[((long long)slot * s.ntdtinv + snap) * s.ncomp + k];
     if (s.format == 1) return (T)(__bfloat162float(((const __nv_bfloat16 *)b)[k * s.n + q]) * sc);
@@ -46,8 +46,9 @@ __device__ __forceinline__ void quant_seg(const KGrid &g, const KState<T> &S, co
     const int i = seg * kSegCells + 2 * lane + 1;
     const bool ok0 = i <= g.nx, ok1 = i + 1 <= g.nx;
     char *b = (char *)sn.base + slot * sn.slot_bytes + hin * sn.snap_bytes;
-    __half *h = (__half *)b;
+    unsigned short *h = (unsigned short *)b;
     float *ex = (float *)(b + sn.ex_off);
+    const bool i16 = sn.format == 4;
     const long long q = (long long)(j - 1) * g.nx + (i - 1);
     for (int t = 0; t < ncomps; t++) {
         const int k = comps[t];
@@ -55,9 +56,9 @@ __device__ __forceinline__ void quant_seg(const KGrid &g, const KState<T> &S, co
         const T *f = fieldp(S, slot, sn.comp_plane[k]);
         const float v0 = ok0 ? (float)f[pidx(g, j, i)] : 0.0f, v1 = ok1 ? (float)f[pidx(g, j, i + 1)] : 0.0f;
         float qf, inv;
-        seg_scales(seg_absmax_warp(v0, v1, ok0, ok1), qf, inv);
-        if (ok0) h[k * sn.n + q] = __float2half_rn(v0 * qf);
-        if (ok1) h[k * sn.n + q + 1] = __float2half_rn(v1 * qf);
+        seg_scales(seg_absmax_warp(v0, v1, ok0, ok1), qf, inv, i16 ? kSegTopI16 : kSegTop);
+        if (ok0) h[k * sn.n + q] = seg_pack(v0 * qf, i16);
+        if (ok1) h[k * sn.n + q + 1] = seg_pack(v1 * qf, i16);
         if (lane == 0) ex[((long long)k * g.ny + (j - 1)) * sn.segs + seg] = inv;
     }
 }
@@ -243,7 +244,8 @@ __device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, floa
     }
 }
 
-template <int PSV, int SH, int AC, bool F16>
+// SEG: 0 fp32 snapshots, 1 fp16 segments, 2 int16 segments
+template <int PSV, int SH, int AC, int SEG>
 __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSnap sn, KGrad gr, int snap) {
     pdl_wait();
     pdl_launch();
@@ -281,16 +283,16 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
         field(P_SXZ, a0.sxz, a1.sxz);
         field(P_SYZ, a0.syz, a1.syz);
     }
-    if constexpr (F16) {
-        // fp16 segments: a pair never straddles a segment (both start at odd i)
-        const __half *hs = (const __half *)sb + q;
+    if constexpr (SEG != 0) {
+        // 16-bit segments: a pair never straddles a segment (both start at odd i)
+        const unsigned short *hs = (const unsigned short *)sb + q;
         const float *ex = (const float *)(sb + sn.ex_off) + (long long)(j - 1) * sn.segs + (i - 1) / kSegCells;
 #pragma unroll
         for (int k = 0; k < NC; k++) {
-            const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(hs + k * sn.n));
+            const unsigned u = *reinterpret_cast<const unsigned *>(hs + k * sn.n);
             const float sc = ex[(long long)k * g.ny * sn.segs];
-            a0.f[k] = v.x * sc;
-            a1.f[k] = v.y * sc;
+            a0.f[k] = seg_unpack((unsigned short)(u & 0xffffu), SEG == 2) * sc;
+            a1.f[k] = seg_unpack((unsigned short)(u >> 16), SEG == 2) * sc;
         }
     } else {
         const float *fs = (const float *)sb + q;

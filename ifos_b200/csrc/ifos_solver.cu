@@ -267,7 +267,7 @@ static int check_params(const ifos_params &p, std::string &why) {
     if (p.seismo < 0 || p.seismo > 5) return bad("SEISMO must be 0..5");
     if (p.max_shots < 1 || p.max_models < 1) return bad("max_shots and max_models must be >= 1");
     if (p.max_src < 0 || p.max_rec < 0) return bad("max_src/max_rec must be >= 0");
-    if (p.snap_format < 0 || p.snap_format > 3) return bad("snap_format must be 0, 1, 2 or 3");
+    if (p.snap_format < 0 || p.snap_format > 4) return bad("snap_format must be 0, 1, 2, 3 or 4");
     if (p.precision < 0 || p.precision > 1) return bad("precision must be 0 or 1");
     if (!(p.dt > 0) || !(p.dh > 0)) return bad("DT and DH must be positive");
     for (int l = 0; l < p.L; l++)
@@ -305,8 +305,8 @@ static Layout layout_of(const ifos_params &p) {
     const int bytes = p.snap_format == 0 ? (p.precision ? 8 : 4) : 2;
     L.snap_bytes_per = (long long)L.ncomp * p.nx * p.ny * bytes;
     L.segs = (p.nx + 63) / 64;
-    if (p.snap_format == IFOS_SNAP_F16S) {
-        // halves [comp][NY*NX], then one fp32 scale per component, row and segment
+    if (p.snap_format == IFOS_SNAP_F16S || p.snap_format == IFOS_SNAP_I16S) {
+        // 16-bit values [comp][NY*NX], then one fp32 scale per component, row and segment
         L.snap_ex_off = (L.snap_bytes_per + 15) / 16 * 16;
         L.snap_bytes_per = (L.snap_ex_off + (long long)L.ncomp * p.ny * L.segs * 4 + 255) / 256 * 256;
     }
@@ -442,7 +442,8 @@ static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     t.snap_ncomp = c->ncomp;
     for (int k = 0; k < NP_FIELD; k++) t.snap_comp[k] = -1;
     for (int k = 0; k < c->ncomp; k++) t.snap_comp[c->comp_plane[k]] = k;
-    c->fused_snap = c->with_snap && (c->p.snap_format == IFOS_SNAP_F32 || c->p.snap_format == IFOS_SNAP_F16S);
+    c->fused_snap = c->with_snap && (c->p.snap_format == IFOS_SNAP_F32 || c->p.snap_format == IFOS_SNAP_F16S ||
+                                     c->p.snap_format == IFOS_SNAP_I16S);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
         c->num_sms = sms;
@@ -923,7 +924,7 @@ struct Launcher {
             so.slot_bytes = c->snap_slot_bytes;
             so.n = (long long)c->p.nx * c->p.ny;
             so.pairs = (c->p.nx % 2) == 0;
-            so.f16 = c->p.snap_format == IFOS_SNAP_F16S;
+            so.f16 = c->p.snap_format == IFOS_SNAP_F16S ? 1 : (c->p.snap_format == IFOS_SNAP_I16S ? 2 : 0);
             so.ex_off = c->snap_ex_off;
             so.segs = (c->p.nx + 63) / 64;
         }
@@ -1206,7 +1207,7 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     // patches the fp32 cells it changes afterwards, and the fp16 segments
     // holding them are stored again after it
     const bool fused = snaps && c->pipe && c->fused_snap;
-    const bool f16s = p.snap_format == IFOS_SNAP_F16S;
+    const bool f16s = p.snap_format == IFOS_SNAP_F16S || p.snap_format == IFOS_SNAP_I16S;  // 16-bit segments
     // P-SV elastic / viscoelastic: the stress kernel applies the explosive
     // sources and the free surface, so nothing changes a stress after it
     // (no surface kernel, no snapshot patches)
@@ -1345,23 +1346,28 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
             KTimer t(c, 3, sample);
             bool pairs = false;
             if constexpr (std::is_same<T, float>::value) {
-                const bool f16s = p.snap_format == IFOS_SNAP_F16S;
-                if ((p.snap_format == IFOS_SNAP_F32 || f16s) && p.nx % 2 == 0) {
+                const bool f16s = p.snap_format == IFOS_SNAP_F16S, i16s = p.snap_format == IFOS_SNAP_I16S;
+                if ((p.snap_format == IFOS_SNAP_F32 || f16s || i16s) && p.nx % 2 == 0) {
                     const dim3 gc((unsigned)((p.nx / 2 + 127) / 128), (unsigned)p.ny, (unsigned)nshots);
                     const int h = ntd - hin_a;
                     auto corr = [&](auto kern) {
                         launch_dep(c->st, c->pdl, kern, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
                     };
                     if (f16s) {
-                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, true>);
-                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, true>);
-                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, true>);
-                        else corr(k_correlate_pairs<0, 1, 0, true>);
+                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, 1>);
+                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 1>);
+                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 1>);
+                        else corr(k_correlate_pairs<0, 1, 0, 1>);
+                    } else if (i16s) {
+                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, 2>);
+                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 2>);
+                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 2>);
+                        else corr(k_correlate_pairs<0, 1, 0, 2>);
                     } else {
-                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, false>);
-                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, false>);
-                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, false>);
-                        else corr(k_correlate_pairs<0, 1, 0, false>);
+                        if (c->ac) corr(k_correlate_pairs<1, 0, 1, 0>);
+                        else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 0>);
+                        else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 0>);
+                        else corr(k_correlate_pairs<0, 1, 0, 0>);
                     }
                     pairs = true;
                 }

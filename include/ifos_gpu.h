@@ -75,6 +75,10 @@ enum {
  * written by the stencil kernels themselves (no extra pass over the
  * wavefield); the scale maps each segment's maximum to 65472. */
 #define IFOS_SNAP_F16S 3
+/* int16 with the scale layout of IFOS_SNAP_F16S: the segment maximum maps to
+ * 32767 and values round to the nearest integer, so the absolute error is at
+ * most about max/65534 (32x below fp16's at the top of a segment) */
+#define IFOS_SNAP_I16S 4
 
 /* Parameters: the reference's global scalars of the propagation path
  * (src/globvar.h; read by src/update_v_PML.c:41-48, src/PML_pro.c:88-98,
