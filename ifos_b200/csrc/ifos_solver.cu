@@ -442,8 +442,9 @@ static void setup_pipeline(ifos_ctx *c, const Layout &L) {
     t.snap_ncomp = c->ncomp;
     for (int k = 0; k < NP_FIELD; k++) t.snap_comp[k] = -1;
     for (int k = 0; k < c->ncomp; k++) t.snap_comp[c->comp_plane[k]] = k;
-    c->fused_snap = c->with_snap && (c->p.snap_format == IFOS_SNAP_F32 || c->p.snap_format == IFOS_SNAP_F16S ||
-                                     c->p.snap_format == IFOS_SNAP_I16S);
+    // int16 segments are stored by k_snap_seg16 after the step, which keeps
+    // their packing out of the stencil kernels
+    c->fused_snap = c->with_snap && (c->p.snap_format == IFOS_SNAP_F32 || c->p.snap_format == IFOS_SNAP_F16S);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
         c->num_sms = sms;
@@ -924,7 +925,7 @@ struct Launcher {
             so.slot_bytes = c->snap_slot_bytes;
             so.n = (long long)c->p.nx * c->p.ny;
             so.pairs = (c->p.nx % 2) == 0;
-            so.f16 = c->p.snap_format == IFOS_SNAP_F16S ? 1 : (c->p.snap_format == IFOS_SNAP_I16S ? 2 : 0);
+            so.f16 = c->p.snap_format == IFOS_SNAP_F16S;
             so.ex_off = c->snap_ex_off;
             so.segs = (c->p.nx + 63) / 64;
         }

@@ -93,7 +93,7 @@ struct KSnapOut {
     long long slot_bytes;  // bytes between slots
     long long n;           // NX*NY
     int pairs;             // NX even: column pairs are aligned for vector stores
-    int f16;               // 16-bit segments: 1 fp16 (IFOS_SNAP_F16S), 2 int16 (IFOS_SNAP_I16S); 0 fp32
+    int f16;               // fp16 segments (IFOS_SNAP_F16S); else fp32
     long long ex_off;      // fp16: bytes from a snapshot to its segment scales [comp][NY][segs]
     int segs;              // fp16: segments per row
 };
@@ -395,10 +395,10 @@ __device__ __forceinline__ void gput2(float *p, float n0, float n1, bool pair, b
 struct RowOut {
     float *st;          // state plane 0 at (j, i)
     float *sn;          // fp32 snapshot component 0 at (j, i), NULL when not storing fp32
-    unsigned short *sh; // 16-bit snapshot component 0 at (j, i), NULL when not storing 16-bit segments
+    __half *sh;         // fp16 snapshot component 0 at (j, i), NULL when not storing fp16
     float *se;          // fp16: scale of component 0 for this row segment
     long long se_comp;  // fp16: scales between components
-    bool pair, v0, spair, i16;
+    bool pair, v0, spair;
     __device__ __forceinline__ RowOut(const KGrid &g, const KState<float> &S, const KSnapOut &so, int slot, int j,
                                       const Cols &cl) {
         st = S.base + (long long)slot * S.slot_stride + ((j - 1 + HY) * g.pitch + (cl.i - 1 + HX));
@@ -406,12 +406,11 @@ struct RowOut {
         sh = nullptr;
         se = nullptr;
         se_comp = 0;
-        i16 = so.f16 == 2;
         if (so.base) {
             char *b = so.base + slot * so.slot_bytes;
             const long long q = (long long)(j - 1) * g.nx + (cl.i - 1);
             if (so.f16) {
-                sh = reinterpret_cast<unsigned short *>(b) + q;
+                sh = reinterpret_cast<__half *>(b) + q;
                 se = reinterpret_cast<float *>(b + so.ex_off) + (long long)(j - 1) * so.segs + (cl.i - 1) / kSegCells;
                 se_comp = (long long)g.ny * so.segs;
             } else {
@@ -435,13 +434,12 @@ struct RowOut {
             }
         } else if (sh) {
             float q, inv;
-            seg_scales(seg_absmax_warp(n0, n1, v0, pair), q, inv, i16 ? kSegTopI16 : kSegTop);
-            unsigned short *p = sh + comp * n;
-            const unsigned short a = seg_pack(n0 * q, i16), b = seg_pack(n1 * q, i16);
-            if (spair) *reinterpret_cast<unsigned *>(p) = (unsigned)a | ((unsigned)b << 16);
+            seg_scales(seg_absmax_warp(n0, n1, v0, pair), q, inv);
+            __half *p = sh + comp * n;
+            if (spair) *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(n0 * q, n1 * q);
             else {
-                if (v0) p[0] = a;
-                if (pair) p[1] = b;
+                if (v0) p[0] = __float2half_rn(n0 * q);
+                if (pair) p[1] = __float2half_rn(n1 * q);
             }
             if (threadIdx.x == 0) se[comp * se_comp] = inv;
         }
