@@ -26,6 +26,7 @@ surface) first.  ``write_model`` writes them in the reference's file order
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -265,17 +266,30 @@ def ricker(p: ShotParams, srcpos: np.ndarray) -> np.ndarray:
 
 
 def write_model(model: dict, prefix: str) -> None:
-    """Write vp/vs/rho as the reference reads them: raw float32, x outer,
-    y inner (src/readmod_elastic.c loop order)."""
-    for key in ("vp", "vs", "rho"):
-        np.ascontiguousarray(model[key].T, dtype=np.float32).tofile(f"{prefix}.{key}")
+    """Write vp/vs/rho (and qp/qs when the model has them) as the reference
+    reads them: raw float32, x outer, y inner (src/readmod_elastic.c,
+    src/readmod.c loop order)."""
+    for key in ("vp", "vs", "rho", "qp", "qs"):
+        if key in model:
+            np.ascontiguousarray(model[key].T, dtype=np.float32).tofile(f"{prefix}.{key}")
 
 
-def read_model(prefix: str, nx: int, ny: int) -> dict:
-    out = {}
-    for key in ("vp", "vs", "rho"):
+def read_model(prefix: str, nx: int, ny: int, tau: float = None) -> dict:
+    """vp, vs, rho as NY x NX planes.  With `tau` (TAU, the viscoelastic
+    reader of src/readmod.c:140-205) also taup and taus: 2/Q from the .qp /
+    .qs files where they exist (the division in double, stored as float),
+    else TAU."""
+    def plane(key):
         a = np.fromfile(f"{prefix}.{key}", dtype=np.float32, count=nx * ny)
-        out[key] = np.ascontiguousarray(a.reshape(nx, ny).T)
+        return np.ascontiguousarray(a.reshape(nx, ny).T)
+
+    out = {key: plane(key) for key in ("vp", "vs", "rho")}
+    if tau is not None:
+        for q, t in (("qp", "taup"), ("qs", "taus")):
+            if os.path.exists(f"{prefix}.{q}"):
+                out[t] = (2.0 / plane(q).astype(np.float64)).astype(np.float32)
+            else:
+                out[t] = np.full((ny, nx), np.float32(tau), np.float32)
     return out
 
 

@@ -150,3 +150,45 @@ def test_seismogram_files_match_saveseis_glob(kind, seismo, wavetype, adjoint_ty
         a = np.fromfile(os.path.join(da, os.path.basename(path)), np.uint8).reshape(ntr, rec)
         b = np.fromfile(path, np.uint8).reshape(ntr, rec)
         assert np.array_equal(a[:, :210], b[:, :210]) and np.array_equal(a[:, 240:], b[:, 240:]), path
+
+
+@pytest.mark.parametrize("with_qs", [True, False])
+def test_viscoelastic_model_reader_matches_readmod(with_qs):
+    """vp, vs, rho and the relaxation planes of a viscoelastic model as
+    src/readmod.c reads them: taup = 2/qp, taus = 2/qs from the .qp / .qs
+    files, TAU where a Q file is missing (the .qs file left out here)."""
+    from ifos_b200 import workloads as W
+    ref, _ = H.libs()
+    rng = np.random.default_rng(21)
+    nx, ny, tau = 13, 9, 0.0731
+    m = {"vp": rng.uniform(1500, 4000, (ny, nx)).astype(np.float32),
+         "vs": rng.uniform(800, 2000, (ny, nx)).astype(np.float32),
+         "rho": rng.uniform(1800, 2600, (ny, nx)).astype(np.float32),
+         "qp": rng.uniform(10, 200, (ny, nx)).astype(np.float32)}
+    if with_qs:
+        m["qs"] = rng.uniform(10, 100, (ny, nx)).astype(np.float32)
+    prefix = os.path.join(tempfile.mkdtemp(prefix="md"), "m")
+    W.write_model(m, prefix)
+    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=1, PARAMETERIZATION=1, L=2, MYID=1, DT=1e-3,
+                  FL=[5.0, 30.0])
+    # IDX / IDY step the write-back loops of src/matrix_operations.c:33-34 (0 would never end)
+    for name, v in (("NXG", nx), ("NYG", ny), ("IDX", 1), ("IDY", 1)):
+        C.c_int.in_dll(ref, name).value = v
+    C.c_float.in_dll(ref, "TAU").value = tau
+    (C.c_char * 74).in_dll(ref, "MFILE").value = prefix.encode()
+    libc = _libc()
+    log = libc.fopen(os.devnull.encode(), b"w")
+    C.c_void_p.in_dll(ref, "FP").value = log
+    mats = [ref.matrix(1, ny, 1, nx) for _ in range(5)]  # rho, pi, u, taus, taup
+    eta = ref.vector(1, 2)
+    f = ref.readmod
+    f.restype = None
+    f.argtypes = [H.FPP] * 5 + [H.FP]
+    f(*mats, eta)
+    libc.fclose(log)
+    want = {k: np.array([[mats[q][j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
+            for q, k in enumerate(("rho", "vp", "vs", "taus", "taup"))}
+    got = W.read_model(prefix, nx, ny, tau=tau)
+    for k, v in want.items():
+        assert np.array_equal(got[k].view(np.int32), v.view(np.int32)), k
+    assert with_qs or (got["taus"] == np.float32(tau)).all()
