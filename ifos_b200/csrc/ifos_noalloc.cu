@@ -1,17 +1,19 @@
 // ifos_dot_f64_noalloc: the FP64 dot product of ifos_dot_f64 for callers that
 // cannot allocate device memory.
 //
-// Some callers of this library cannot call cudaMalloc: code that runs inside
-// a host callback or a real-time loop where an allocation would synchronise
-// the device or stall, code whose GPU memory is owned and fully budgeted by
-// another framework, or a pre-allocated inversion driver that must not
-// fragment device memory between iterations.  They can still reduce data they
-// already hold on the device.  This entry point needs no context and touches
-// no allocator: its scratch (one partial sum per block plus the result) lives
-// in the file-scope array below, which every GPU that loads the library holds
-// until the process exits.
+// Some callers of this library cannot call cudaMalloc: code whose GPU memory
+// is owned and fully budgeted by another framework (a caching allocator that
+// has already reserved the device), a latency-bound loop where cudaMalloc or
+// cudaFree would synchronise the whole device, or a pre-allocated inversion
+// driver that must not fragment device memory between iterations.  They can
+// still reduce data they already hold on the device.  This entry point needs
+// no context and touches no allocator: its scratch (one partial sum per block
+// plus the result) lives in the file-scope array below, which every GPU that
+// loads the library holds until the process exits.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 
 #include "ifos_gpu.h"
@@ -34,7 +36,20 @@ constexpr int kMaxDevices = 64;
 
 // Device address of g_scratch per device, looked up once with that device
 // current (host code must not use the symbol itself as a device pointer).
-double *g_scratch_dev[kMaxDevices] = {nullptr};
+// Threads making their first call at the same time serialise on the mutex;
+// later calls read the published address without locking.
+std::atomic<double *> g_scratch_dev[kMaxDevices];
+std::mutex g_scratch_mu;
+
+// Restores the calling thread's current device on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    DeviceGuard() { ok = cudaGetDevice(&prev) == cudaSuccess; }
+    ~DeviceGuard() {
+        if (ok) cudaSetDevice(prev);
+    }
+};
 
 __global__ void k_partial(const float *a, const float *b, long long n, double *scratch) {
     double acc = 0.0;
@@ -79,24 +94,32 @@ extern "C" int ifos_dot_f64_noalloc(int device, const float *a, const float *b, 
                                     double *out) {
     if (!a || !out) return fail(IFOS_ERR_ARG, "ifos_dot_f64_noalloc: null input or output");
     if (device < 0 || device >= kMaxDevices) return fail(IFOS_ERR_ARG, "ifos_dot_f64_noalloc: bad device index");
-    const long long max_n = (long long)kMaxBlocks * kThreads * kPerThread;
-    if ((long long)n > max_n)
+    // compared unsigned: a count that wrapped (a negative value through an
+    // unsigned parameter) is rejected too, before any launch
+    const size_t max_n = (size_t)kMaxBlocks * kThreads * kPerThread;
+    if (n > max_n)
         return fail(IFOS_ERR_ARG, "ifos_dot_f64_noalloc: n = " + std::to_string(n) + " exceeds the maximum of " +
                                       std::to_string(max_n) + " elements (" + std::to_string(kMaxBlocks) +
                                       " partial sums of the static scratch)");
+    DeviceGuard guard;
+    if (!guard.ok) return fail(IFOS_ERR_CUDA, "ifos_dot_f64_noalloc: cudaGetDevice failed");
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(IFOS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
-    if (!g_scratch_dev[device]) {
+    double *scratch = g_scratch_dev[device].load(std::memory_order_acquire);
+    if (!scratch) {
         // first call on this device: resolve the scratch address (before any capture)
-        double *ptr = nullptr;
-        e = cudaGetSymbolAddress((void **)&ptr, g_scratch);
-        if (e != cudaSuccess || !ptr)
-            return fail(IFOS_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch: ") + cudaGetErrorString(e));
-        g_scratch_dev[device] = ptr;
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        scratch = g_scratch_dev[device].load(std::memory_order_relaxed);
+        if (!scratch) {
+            e = cudaGetSymbolAddress((void **)&scratch, g_scratch);
+            if (e != cudaSuccess || !scratch)
+                return fail(IFOS_ERR_CUDA,
+                            std::string("cudaGetSymbolAddress of the scratch: ") + cudaGetErrorString(e));
+            g_scratch_dev[device].store(scratch, std::memory_order_release);
+        }
     }
-    double *scratch = g_scratch_dev[device];
     cudaStream_t st = (cudaStream_t)stream;
-    const long long per_block = (long long)kThreads * kPerThread;
+    const size_t per_block = (size_t)kThreads * kPerThread;
     int nb = (int)((n + per_block - 1) / per_block);
     if (nb < 1) nb = 1;
     k_partial<<<nb, kThreads, 0, st>>>(a, b, (long long)n, scratch);

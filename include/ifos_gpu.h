@@ -357,19 +357,22 @@ int ifos_mat_change_test(ifos_ctx *ctx, const ifos_mat_change *mc, float *vp, fl
 int ifos_opt_step(const float *l2t, const float *epst, int fp64, float *opteps);
 
 /* FP64 dot product without any device allocation.  No counterpart in the
- * reference: it is for callers that cannot call cudaMalloc (code running in
- * host callbacks or latency-bound loops where an allocation would stall, or
- * whose device memory is fully budgeted by another framework) and already hold
- * the data on the device.  Returns sum(a*b) (b NULL: sum(a*a)) over n floats
- * at DEVICE pointers a, b of `device`, accumulated in double, in *out (host).
- * Needs no context.  Its scratch is a static array of IFOS_NOALLOC_MAX_BLOCKS+1
- * doubles that every device loading the library keeps until exit; n is
- * limited to IFOS_NOALLOC_MAX_N (IFOS_ERR_ARG above it, message in
- * ifos_last_error(NULL)).  The first call on a device resolves the scratch
- * address and should come before any stream capture.  Launches go to `stream`
- * (NULL: the default stream) and the call returns after the result is copied.
- * All calls on a device share the scratch, so calls that overlap on the GPU
- * (other host threads, other streams) race. */
+ * reference: it is for callers that cannot call cudaMalloc -- code whose
+ * device memory is owned and fully budgeted by another framework, or a
+ * latency-bound loop where an allocation would synchronise the device -- and
+ * already hold the data on the device.  Returns sum(a*b) (b NULL: sum(a*a))
+ * over n floats at DEVICE pointers a, b of `device`, accumulated in double,
+ * in *out (host).  Needs no context.  Its scratch is a static array of
+ * IFOS_NOALLOC_MAX_BLOCKS+1 doubles that every device loading the library
+ * keeps until exit; n is limited to IFOS_NOALLOC_MAX_N (IFOS_ERR_ARG above
+ * it, message in ifos_last_error(NULL)).  The first call on a device resolves
+ * the scratch address and should come before any stream capture.  Launches
+ * go to `stream` (NULL: the default stream); the call copies the result to
+ * host memory and waits for `stream` before it returns, so it must not be
+ * called from a host function enqueued on a stream.  The calling thread's
+ * current device is restored before returning.  All calls on a device share
+ * the scratch, so calls that overlap on the GPU (other host threads, other
+ * streams) race. */
 #define IFOS_NOALLOC_MAX_BLOCKS 4096
 #define IFOS_NOALLOC_MAX_N (4096LL * 256 * 32)
 int ifos_dot_f64_noalloc(int device, const float *a, const float *b, size_t n, void *stream, double *out);

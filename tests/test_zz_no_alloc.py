@@ -1,13 +1,15 @@
 """The allocation-free FP64 dot product, ifos_dot_f64_noalloc.
 
 It serves callers that cannot call cudaMalloc themselves or through the
-library -- code in host callbacks or latency-bound loops where an allocation
-would stall the device, or code whose device memory is fully budgeted by
-another framework -- but already hold their data on the GPU.  Its scratch is
-a static device array, so the test checks what sharing that array implies:
-two calls in a row (the second must not see the first's partial sums), each
-against the existing entry point ifos_dot_f64 within the tolerance the other
-reduction tests use, and a clear rejection of sizes beyond the array.
+library -- code whose device memory is fully budgeted by another framework,
+or a latency-bound loop where an allocation would synchronise the device --
+but already hold their data on the GPU.  Its scratch is a static device
+array, so the test checks what sharing that array implies: two calls in a
+row (the second must not see the first's partial sums), each against the
+existing entry point ifos_dot_f64 and against numpy in fp64 within the
+tolerance the other reduction tests use, the caller's current device left as
+it was, and a clear rejection of sizes beyond the array (including a count
+that wrapped around).
 
 This file sorts last so that a run stopping at the first failure has run
 every other test already; it also passes on its own in a fresh process.
@@ -53,6 +55,11 @@ def test_noalloc_dot_matches_existing_entry_point_twice_in_a_row():
     scale1 = float(np.dot(a1.astype(np.float64), a1.astype(np.float64)))
     assert abs(got1 - ref1) < 1e-9 * scale1, (got1, ref1)
     assert abs(got2 - ref2) < 1e-9 * ref2, (got2, ref2)
+    np1 = float(np.dot(a1.astype(np.float64), b1.astype(np.float64)))
+    np2 = float(np.dot(a2.astype(np.float64), a2.astype(np.float64)))
+    assert abs(got1 - np1) < 1e-9 * scale1, (got1, np1)
+    assert abs(got2 - np2) < 1e-9 * np2, (got2, np2)
+    assert torch.cuda.current_device() == 0
     # and again with the first input: no state carried over from the larger call
     rc, again = _noalloc(lib, da1.data_ptr(), db1.data_ptr(), n1)
     assert rc == 0 and again == got1
@@ -65,5 +72,9 @@ def test_noalloc_dot_rejects_sizes_beyond_its_scratch():
     tiny = torch.zeros(4, device="cuda")
     too_many = 4096 * 256 * 32 + 1  # IFOS_NOALLOC_MAX_N + 1; rejected before any launch
     rc, _ = _noalloc(lib, tiny.data_ptr(), None, too_many)
+    assert rc == 1
+    assert b"exceeds the maximum" in lib.ifos_last_error(None)
+    # a negative count passed through the unsigned size parameter
+    rc, _ = _noalloc(lib, tiny.data_ptr(), None, C.c_size_t(-1).value)
     assert rc == 1
     assert b"exceeds the maximum" in lib.ifos_last_error(None)
