@@ -57,42 +57,187 @@ class Geometry:
     recpos: np.ndarray
 
 
+def _ctrunc_div(a: int, b: int) -> int:
+    """C integer division (truncates toward zero)."""
+    q = abs(a) // abs(b)
+    return q if (a >= 0) == (b > 0) else -q
+
+
+def _crem(a: int, b: int) -> int:
+    """C remainder (sign of the dividend)."""
+    return a - _ctrunc_div(a, b) * b
+
+
+def _grid_index(coord_m, dh) -> int:
+    """iround(coord / DH) in float arithmetic, the reference's macro
+    ((int)floor(x + 0.5), src/fd.h:15) applied to a float quotient."""
+    return iround(float(np.float32(np.float32(coord_m) / np.float32(dh))))
+
+
+def split_sources(p: ShotParams, srcpos: np.ndarray) -> np.ndarray:
+    """Local source rows of a single-rank run as src/splitsrc.c:33-50 forms
+    them from the global srcpos (8 x nsrc, positions in metres, the rows of
+    src/sources.c): a source is kept when (iround(x/DH)-1)/NX and
+    (iround(y/DH)-1)/NY are 0 in C's truncating division -- sources right of
+    or below the grid are dropped -- and its indices are
+    ((iround(x/DH)-1) % NX) + 1 with C's remainder, so cell 0 stays 0."""
+    rows = []
+    for l in range(srcpos.shape[1]):
+        ix = _grid_index(srcpos[0, l], p.dh)
+        iy = _grid_index(srcpos[1, l], p.dh)
+        if _ctrunc_div(ix - 1, p.nx) != 0 or _ctrunc_div(iy - 1, p.ny) != 0:
+            continue
+        r = np.zeros(8, np.float32)
+        r[0] = _crem(ix - 1, p.nx) + 1
+        r[1] = _crem(iy - 1, p.ny) + 1
+        r[3:8] = srcpos[3:8, l]
+        rows.append(r)
+    return np.stack(rows, axis=1) if rows else np.zeros((8, 0), np.float32)
+
+
 def source_rows(p: ShotParams, xs_m, ys_m, fc, amp=1.0, tshift=0.0, azimuth=0.0, stype=None) -> np.ndarray:
     """Grid-located sources as ``splitsrc`` produces them for one rank
-    (src/splitsrc.c:35-50): index = iround(x/DH) in float arithmetic."""
+    (src/splitsrc.c:33-50) from positions in metres."""
     xs_m = np.atleast_1d(np.asarray(xs_m, np.float32))
     ys_m = np.atleast_1d(np.asarray(ys_m, np.float32))
-    n = xs_m.size
-    rows = np.zeros((8, n), np.float32)
-    dh = np.float32(p.dh)
-    for l in range(n):
-        ix = iround(float(np.float32(xs_m[l] / dh)))
-        iy = iround(float(np.float32(ys_m[l] / dh)))
-        rows[0, l] = ((ix - 1) % p.nx) + 1 if ix >= 1 else ix
-        rows[1, l] = ((iy - 1) % p.ny) + 1 if iy >= 1 else iy
-        rows[3, l] = tshift
-        rows[4, l] = fc
-        rows[5, l] = amp
-        rows[6, l] = azimuth
-        rows[7, l] = p.source_type if stype is None else stype
-    return rows
+    g = np.zeros((8, xs_m.size), np.float32)
+    g[0], g[1] = xs_m, ys_m
+    g[3], g[4], g[5], g[6] = tshift, fc, amp, azimuth
+    g[7] = p.source_type if stype is None else stype
+    return split_sources(p, g)
+
+
+def _scan_floats(text: str, count: int):
+    """Up to `count` leading floats of `text` as sscanf's %f conversions read
+    them (whitespace-separated, stopping at the first that does not parse),
+    each rounded once to float32 as strtof rounds it."""
+    out = []
+    for tok in text.split():
+        if len(out) == count:
+            break
+        try:
+            out.append(_strtof(tok))
+        except ValueError:
+            break
+    return out
+
+
+def _strtof(tok: str) -> np.float32:
+    """Decimal string to float32 with one rounding (strtof), not through a
+    double (which can round twice)."""
+    import ctypes
+    global _LIBC_STRTOF
+    if _LIBC_STRTOF is None:
+        libc = ctypes.CDLL(None)
+        _LIBC_STRTOF = libc.strtof
+        _LIBC_STRTOF.restype = ctypes.c_float
+        _LIBC_STRTOF.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p)]
+    b = tok.encode()
+    end = ctypes.c_char_p()
+    v = _LIBC_STRTOF(b, ctypes.byref(end))
+    if ctypes.cast(end, ctypes.c_void_p).value == ctypes.cast(ctypes.c_char_p(b), ctypes.c_void_p).value:
+        raise ValueError(tok)
+    return np.float32(v)
+
+
+_LIBC_STRTOF = None
+
+
+def read_source_file(path: str, source_type: int) -> np.ndarray:
+    """Global source table of a SOURCE_FILE as src/sources.c:45-96 reads it:
+    the first line's leading integer is the count; each following line holds
+    x, z (ignored), y, tshift, fc, amp, azimuth, type.  A line with fewer than
+    six values is an error (the reference declares one); azimuth defaults to
+    0 and the type to SOURCE_TYPE.  Returns 8 x nsrc rows in the srcpos
+    layout (x, y, 0, tshift, fc, amp, azimuth, type; positions in metres)."""
+    with open(path, "rb") as fh:
+        lines = fh.read().decode("latin-1").split("\n")
+    nsrc = int(lines[0].split()[0])
+    out = np.zeros((8, nsrc), np.float32)
+    for l in range(nsrc):
+        line = lines[1 + l] if 1 + l < len(lines) else ""
+        v = _scan_floats(line[:254], 8)
+        if len(v) < 6:
+            raise ValueError(f"{path}: source {l + 1} has {len(v)} values; x, z, y, tshift, fc and amp are required")
+        out[0, l], out[1, l], out[3, l] = v[0], v[2], v[3]
+        out[4, l], out[5, l] = v[4], v[5]
+        out[6, l] = v[6] if len(v) > 6 else 0.0
+        out[7, l] = v[7] if len(v) > 7 else source_type
+    return out
+
+
+def read_receiver_file(path: str, p: ShotParams) -> np.ndarray:
+    """Global receiver grid indices of a REC_FILE as src/receiver.c:47-93
+    (READREC=1) forms them: as many (x, y) pairs as the file has newline
+    characters, each read like fscanf("%f%f\n") (a pair that cannot be read
+    keeps the previous values), index iround((x + REFREC)/DH) in float
+    arithmetic; a receiver on the same cell as an earlier one is dropped, as
+    is one whose x index is not positive.  Returns 2 x ntr (int32)."""
+    with open(path, "rb") as fh:
+        data = fh.read().decode("latin-1")
+    ntr1 = data.count("\n")
+    toks = data.split()
+    pos, x, y = 0, np.float32(0), np.float32(0)
+    dh, rx, ry = np.float32(p.dh), np.float32(p.refrecx), np.float32(p.refrecy)
+    cells = []
+    for _ in range(ntr1):
+        for k in range(2):
+            if pos >= len(toks):
+                break
+            try:
+                v = _strtof(toks[pos])
+            except ValueError:
+                pos = len(toks)  # fscanf stays stuck on a token that does not parse
+                break
+            pos += 1
+            if k == 0:
+                x = v
+            else:
+                y = v
+        cells.append([iround(float(np.float32((x + rx) / dh))), iround(float(np.float32((y + ry) / dh)))])
+    # duplicates are marked with negative x in file order (src/receiver.c:73-78)
+    flag = 0
+    for a in range(len(cells) - 1):
+        for b in range(a + 1, len(cells)):
+            if cells[a][0] == cells[b][0] and cells[a][1] == cells[b][1]:
+                flag += 1
+                cells[b][0] = -flag
+    kept = [c for c in cells if c[0] > 0]
+    return np.array(kept, np.int32).T.copy() if kept else np.zeros((2, 0), np.int32)
+
+
+def split_receivers(p: ShotParams, recpos: np.ndarray):
+    """Local receivers of a single-rank run as src/splitrec.c:38-60 selects
+    them: (ix-1)/NX and (iy-1)/NY must be 0 in C's truncating division, the
+    local index is ((i-1) % N) + 1 with C's remainder.  Returns (2 x ntr_loc
+    int32, recswitch per global receiver)."""
+    out, sw = [], np.zeros(recpos.shape[1], np.int32)
+    for k in range(recpos.shape[1]):
+        ix, iy = int(recpos[0, k]), int(recpos[1, k])
+        if _ctrunc_div(ix - 1, p.nx) != 0 or _ctrunc_div(iy - 1, p.ny) != 0:
+            continue
+        sw[k] = 1
+        out.append((_crem(ix - 1, p.nx) + 1, _crem(iy - 1, p.ny) + 1))
+    return (np.array(out, np.int32).T.copy() if out else np.zeros((2, 0), np.int32)), sw
 
 
 def receiver_rows(p: ShotParams, xr_m, yr_m) -> np.ndarray:
-    """Receiver grid indices as ``receiver`` computes them from a file
-    (src/receiver.c:58-60, float parse then iround((x+REFREC)/DH)) with
-    same-cell duplicates removed in file order (src/receiver.c:73-88)."""
+    """Local receiver grid indices of receivers at positions in metres, as
+    ``receiver`` and ``splitrec`` form them for one rank (float
+    iround((x+REFREC)/DH), same-cell duplicates removed in file order,
+    receivers off the grid dropped)."""
     dh = np.float32(p.dh)
-    out = []
+    rx, ry = np.float32(p.refrecx), np.float32(p.refrecy)
+    cells = []
     seen = set()
     for x, y in zip(np.asarray(xr_m, np.float32), np.asarray(yr_m, np.float32)):
-        ix = iround(float(np.float32((x + np.float32(p.refrecx)) / dh)))
-        iy = iround(float(np.float32((y + np.float32(p.refrecy)) / dh)))
-        if (ix, iy) in seen:
+        c = (iround(float(np.float32((x + rx) / dh))), iround(float(np.float32((y + ry) / dh))))
+        if c in seen or c[0] <= 0:
             continue
-        seen.add((ix, iy))
-        out.append((ix, iy))
-    return np.array(out, np.int32).T.copy()
+        seen.add(c)
+        cells.append(c)
+    rec = np.array(cells, np.int32).T.copy() if cells else np.zeros((2, 0), np.int32)
+    return split_receivers(p, rec)[0]
 
 
 # ----------------------------------------------------------------------------
@@ -274,18 +419,29 @@ def write_model(model: dict, prefix: str) -> None:
             np.ascontiguousarray(model[key].T, dtype=np.float32).tofile(f"{prefix}.{key}")
 
 
-def read_model(prefix: str, nx: int, ny: int, tau: float = None) -> dict:
+def read_model(prefix: str, nx: int, ny: int, tau: float = None, wavetype: int = 1) -> dict:
     """vp, vs, rho as NY x NX planes.  With `tau` (TAU, the viscoelastic
     reader of src/readmod.c:140-205) also taup and taus: 2/Q from the .qp /
     .qs files where they exist (the division in double, stored as float),
-    else TAU."""
+    else TAU.  As src/readmod.c:59-77 and :146-160 do, the .vp / .qp files
+    and taup are read only for WAVETYPE 1 (P-SV) and 3 (both): an SH model
+    (wavetype 2) needs no .vp file.  A file that does not hold exactly NX*NY
+    values raises ValueError, where the reference stops at its feof checks
+    ("to small", :148-181; "to big", :210-245).  One difference: the
+    reference's checks run before each read, so a file short by exactly one
+    value passes them there (the last cell keeps the previous value) and is
+    rejected here."""
     def plane(key):
-        a = np.fromfile(f"{prefix}.{key}", dtype=np.float32, count=nx * ny)
+        a = np.fromfile(f"{prefix}.{key}", dtype=np.float32)
+        if a.size != nx * ny:
+            raise ValueError(f"model file {prefix}.{key} is too {'small' if a.size < nx * ny else 'big'}: "
+                             f"{a.size} values, NX*NY = {nx * ny}")
         return np.ascontiguousarray(a.reshape(nx, ny).T)
 
-    out = {key: plane(key) for key in ("vp", "vs", "rho")}
+    psv = wavetype in (1, 3)
+    out = {key: plane(key) for key in (("vp", "vs", "rho") if psv else ("vs", "rho"))}
     if tau is not None:
-        for q, t in (("qp", "taup"), ("qs", "taus")):
+        for q, t in ((("qp", "taup"),) if psv else ()) + (("qs", "taus"),):
             if os.path.exists(f"{prefix}.{q}"):
                 out[t] = (2.0 / plane(q).astype(np.float64)).astype(np.float32)
             else:

@@ -152,11 +152,12 @@ def test_seismogram_files_match_saveseis_glob(kind, seismo, wavetype, adjoint_ty
         assert np.array_equal(a[:, :210], b[:, :210]) and np.array_equal(a[:, 240:], b[:, 240:]), path
 
 
-@pytest.mark.parametrize("with_qs", [True, False])
-def test_viscoelastic_model_reader_matches_readmod(with_qs):
+@pytest.mark.parametrize("with_qs,wavetype", [(True, 1), (False, 1), (True, 2)])
+def test_viscoelastic_model_reader_matches_readmod(with_qs, wavetype):
     """vp, vs, rho and the relaxation planes of a viscoelastic model as
     src/readmod.c reads them: taup = 2/qp, taus = 2/qs from the .qp / .qs
-    files, TAU where a Q file is missing (the .qs file left out here)."""
+    files, TAU where a Q file is missing (the .qs file left out here).  An SH
+    model (WAVETYPE 2) has no .vp / .qp file and no taup plane."""
     from ifos_b200 import workloads as W
     ref, _ = H.libs()
     rng = np.random.default_rng(21)
@@ -167,9 +168,11 @@ def test_viscoelastic_model_reader_matches_readmod(with_qs):
          "qp": rng.uniform(10, 200, (ny, nx)).astype(np.float32)}
     if with_qs:
         m["qs"] = rng.uniform(10, 100, (ny, nx)).astype(np.float32)
+    if wavetype == 2:
+        del m["vp"], m["qp"]
     prefix = os.path.join(tempfile.mkdtemp(prefix="md"), "m")
     W.write_model(m, prefix)
-    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=1, PARAMETERIZATION=1, L=2, MYID=1, DT=1e-3,
+    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=wavetype, PARAMETERIZATION=1, L=2, MYID=1, DT=1e-3,
                   FL=[5.0, 30.0])
     # IDX / IDY step the write-back loops of src/matrix_operations.c:33-34 (0 would never end)
     for name, v in (("NXG", nx), ("NYG", ny), ("IDX", 1), ("IDY", 1)):
@@ -187,8 +190,27 @@ def test_viscoelastic_model_reader_matches_readmod(with_qs):
     f(*mats, eta)
     libc.fclose(log)
     want = {k: np.array([[mats[q][j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
-            for q, k in enumerate(("rho", "vp", "vs", "taus", "taup"))}
-    got = W.read_model(prefix, nx, ny, tau=tau)
+            for q, k in enumerate(("rho", "vp", "vs", "taus", "taup")) if wavetype != 2 or k not in ("vp", "taup")}
+    got = W.read_model(prefix, nx, ny, tau=tau, wavetype=wavetype)
+    assert sorted(got) == sorted(want)
     for k, v in want.items():
         assert np.array_equal(got[k].view(np.int32), v.view(np.int32)), k
     assert with_qs or (got["taus"] == np.float32(tau)).all()
+
+
+def test_model_reader_rejects_files_of_the_wrong_size():
+    """A model file with fewer or more than NX*NY values is an error, as the
+    feof checks of src/readmod.c:146-245 make it."""
+    from ifos_b200 import workloads as W
+    nx, ny = 7, 5
+    d = tempfile.mkdtemp(prefix="md")
+    prefix = os.path.join(d, "m")
+    m = {k: np.full((ny, nx), 1000.0, np.float32) for k in ("vp", "vs", "rho")}
+    W.write_model(m, prefix)
+    W.read_model(prefix, nx, ny)
+    np.zeros(nx * ny - 3, np.float32).tofile(prefix + ".vs")
+    with pytest.raises(ValueError, match="too small"):
+        W.read_model(prefix, nx, ny)
+    np.zeros(nx * ny + 1, np.float32).tofile(prefix + ".vs")
+    with pytest.raises(ValueError, match="too big"):
+        W.read_model(prefix, nx, ny)
