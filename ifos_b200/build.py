@@ -16,11 +16,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libifos_b200.so")
-SOURCES = ["ifos_solver.cu", "ifos_setup.cpp", "ifos_noalloc.cu"]
+SOURCES = ["ifos_solver.cu", "ifos_setup.cpp", "ifos_noalloc.cu", "ifos_pipe.cu"]
+# ifos_pipe.cu is compiled once per half stencil width (-DIFOS_PIPE_FD=1..6)
+PIPE_SRC = "ifos_pipe.cu"
+PIPE_WIDTHS = range(1, 7)
+OBJ_DIR = os.path.join(HERE, "_build")
 # the reference-named per-kernel entry points; the driver defines the globals they read
 LIB_COMPAT = os.path.join(HERE, "libifos_compat.so")
 SOURCES_COMPAT = ["ifos_compat.cu"]
-HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h", "ifos_tma.cuh", "ifos_tile.cuh"]
+HEADERS = ["ifos_kernels.cuh", "ifos_snap.cuh", "ifos_setup.h", "ifos_tma.cuh", "ifos_tile.cuh", "ifos_launch.cuh",
+           "ifos_update.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -56,14 +61,40 @@ def up_to_date(lib=LIB, sources=SOURCES, header="ifos_gpu.h") -> bool:
         return fh.read().strip() == _digest(sources, header)
 
 
+def _units(sources):
+    """(source, extra defines, object name) of every translation unit."""
+    out = []
+    for src in sources:
+        stem = os.path.splitext(src)[0]
+        if src == PIPE_SRC:
+            out += [(src, [f"-DIFOS_PIPE_FD={fd}"], f"{stem}_fd{fd}.o") for fd in PIPE_WIDTHS]
+        else:
+            out.append((src, [], stem + ".o"))
+    return out
+
+
 def _compile(lib, sources, verbose, extra, header="ifos_gpu.h"):
+    """Compile every translation unit to an object in parallel, then link."""
     stamp = _digest(sources, header) if not extra else None
-    cmd = [nvcc(), "-O3", *ARCH, "-lineinfo", "--fmad=false", "-std=c++17", "-shared",
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", lib + ".tmp", *[os.path.join(CSRC, s) for s in sources], "-lcudart", *extra]
+    common = [nvc := nvcc(), "-O3", *ARCH, "-lineinfo", "--fmad=false", "-std=c++17",
+              "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+    odir = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(lib))[0])
+    os.makedirs(odir, exist_ok=True)
+    procs, objs = [], []
+    for src, defs, obj in _units(sources):
+        o = os.path.join(odir, obj)
+        cmd = common + defs + ["-c", os.path.join(CSRC, src), "-o", o, *extra]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((subprocess.Popen(cmd), cmd))
+        objs.append(o)
+    failed = [cmd for p, cmd in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    link = [nvc, *ARCH, "-shared", "-o", lib + ".tmp", *objs, "-lcudart"]
     if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        print(" ".join(link), file=sys.stderr)
+    subprocess.run(link, check=True)
     os.replace(lib + ".tmp", lib)
     if stamp:
         with open(lib + ".stamp", "w") as fh:

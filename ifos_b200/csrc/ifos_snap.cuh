@@ -384,6 +384,10 @@ __global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int 
     }
 }
 
+// The host-called kernels below are compiled into the solver unit only (the
+// per-width stencil units define IFOS_PIPE_FD and do not launch them).
+#ifndef IFOS_PIPE_FD
+
 // sum of the assembled gradients over slots (src/IFOS2D.c:2703-2724), in slot
 // order so the float additions match the reference's shot loop
 __global__ void k_grad_sum(const float *grads, int nshots, long long n, float *out) {
@@ -693,4 +697,5 @@ __global__ void k_median_smooth(const float *in, float *out, int nx, int ny, int
     out[q] = t[k / 2 + 1];
 }
 
+#endif  // IFOS_PIPE_FD
 }  // namespace ifos

@@ -531,7 +531,7 @@ template <int LL>
 struct RowVals {
     float sxx[2], syy[2], p[LL > 0 ? LL : 1][2], q[LL > 0 ? LL : 1][2];
 };
-__device__ __noinline__ float4 psource_row_v(const KGrid &g, const KSrc &src, int slot, int nt, int j, Cols cl,
+static __device__ __noinline__ float4 psource_row_v(const KGrid &g, const KSrc &src, int slot, int nt, int j, Cols cl,
                                              float4 v) {
     float sxx[2] = {v.x, v.y}, syy[2] = {v.z, v.w};
     psource_row(g, src, slot, nt, j, cl, sxx, syy);
