@@ -85,23 +85,30 @@ def workload(nt):
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes of the stress kernel per launch (per cell: v read 8,
-# stress read+write 24, L memory triples read+write 24L, six coefficient
-# planes 24; each CPML strip cell reads+writes two psi values: 16 B)
-def stress_bytes(p):
-    n = p.nx * p.ny
-    per_cell = 8 + 24 + 24 * p.L + 24
-    strip_cells = 2 * p.fw * p.ny + p.fw * p.nx * (1 if p.free_surf else 2)
-    return n * per_cell + strip_cells * 16
+# Algorithmic bytes of the stress kernel per launch.  Per cell and shot: v
+# read 8, stress read+write 24, L memory triples read+write 24L; each CPML
+# strip cell reads+writes two psi values (16 B).  The six coefficient planes
+# (24 B per cell) belong to the model: a launch over B shots of one model
+# reads them once (the shots' tiles are neighbours in the tile order), so the
+# honest count charges them once per distinct model; the per-shot count
+# charges them once per shot.
+def _strip_cells(p):
+    return 2 * p.fw * p.ny + p.fw * p.nx * (1 if p.free_surf else 2)
 
 
-# velocity kernel: stresses read 12, velocities read+write 16, rip/rjp 8,
-# (adjoint: the time integrals of the velocity read+write 16)
-def velocity_bytes(p, adjoint):
+def stress_bytes(p, shots=1, models=1, per_shot_model=False):
     n = p.nx * p.ny
-    per_cell = 12 + 16 + 8 + (16 if adjoint else 0)
-    strip_cells = 2 * p.fw * p.ny + p.fw * p.nx * (1 if p.free_surf else 2)
-    return n * per_cell + strip_cells * 16
+    state = n * (8 + 24 + 24 * p.L) + _strip_cells(p) * 16
+    coeff = n * 24
+    return shots * state + (shots if per_shot_model else models) * coeff
+
+
+# velocity kernel: stresses read 12, velocities read+write 16, (adjoint: the
+# time integrals of the velocity read+write 16) per shot; rip/rjp 8 per model
+def velocity_bytes(p, adjoint, shots=1, models=1):
+    n = p.nx * p.ny
+    state = n * (12 + 16 + (16 if adjoint else 0)) + _strip_cells(p) * 16
+    return shots * state + models * n * 8
 
 
 def measured_peak():
@@ -113,27 +120,35 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def library_stamp():
+    """First 16 hex digits of the stamp of the built solver library (the hash
+    of its sources and flags)."""
+    try:
+        with open(os.path.join(ROOT, "ifos_b200", "libifos_b200.so.stamp")) as fh:
+            return fh.read().strip()[:16]
+    except OSError:
+        return None
+
+
 def ncu_traffic(shots):
     """DRAM bytes per launch of the stress kernel from the committed ncu
     summaries (profiles/ncu_traffic.txt: `stress_visco_fp32 <bytes> <cells>
-    <shots per launch>`): the capture with the same shots per launch, else
-    the single-shot capture scaled by shots.  Returns (bytes for one launch
-    of `cells`-cell shots, note)."""
+    <shots per launch> <library stamp>`), used only when the stamp matches
+    the library this run loads: a capture of another build says nothing about
+    this one.  Returns (bytes, cells, note) or None."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    stamp = library_stamp()
     rows = []
     try:
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 4 and parts[0] == "stress_visco_fp32":
+            if len(parts) >= 5 and parts[0] == "stress_visco_fp32" and parts[4] == stamp:
                 rows.append((float(parts[1]), float(parts[2]), int(parts[3])))
     except OSError:
         pass
     for b, c, s in rows:
         if s == shots:
-            return b, c, f"ncu capture of a {s}-shot launch"
-    for b, c, s in rows:
-        if s == 1:
-            return b * shots, c, f"ncu capture of a 1-shot launch, scaled by {shots} shots"
+            return b, c, f"ncu capture of a {s}-shot launch of this build ({stamp})"
     return None
 
 
@@ -246,34 +261,42 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def fp64_error(p, model, g, nt=300):
-    """Error of the fp32 path and of each snapshot format against the same
-    kernels in fp64 arithmetic with fp64 snapshots, on a truncated run of the
-    workload grid (untimed)."""
+def fp64_error(p, model, g, nt=None, formats=("fp32", "fp16s"), device=0):
+    """Error of the fp32 path and of snapshot formats against the same
+    kernels in fp64 arithmetic with fp64 snapshots, on one shot of the
+    workload at its own NT by default (untimed).  The misfit is the FP64
+    device misfit of the residual against seeded observed data, and the
+    adjoint is driven by that residual, as in the timed steps."""
     from ifos_b200 import workloads as W
     from ifos_b200.solver import ShotSolver
-    q = p.copy(nt=nt)
+    q = p.copy(nt=nt) if nt and nt != p.nt else p
     sig = W.ricker(q, g.srcpos)
     ntr = g.recpos.shape[1]
     rng = np.random.default_rng(1)
-    adj = (rng.standard_normal((1, 3, ntr, nt)) * 1e-6).astype(np.float32)
+    obs = (rng.standard_normal((1, 3, ntr, q.nt)) * 1e-9).astype(np.float32)
     out = {}
-    for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
-                    ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s")),
-                    ("i16s", dict(snap_format="i16s"))):
-        with ShotSolver(q, max_rec=ntr, **kw) as s:
+    for tag in ("fp64",) + tuple(formats):
+        kw = dict(precision="fp64") if tag == "fp64" else ({} if tag == "fp32" else dict(snap_format=tag))
+        with ShotSolver(q, max_rec=ntr, device=device, **kw) as s:
             s.upload_model(model)
             s.setup_shot(0, g.srcpos, sig, g.recpos)
             sec = s.forward(1, store=True)[0]
-            gr = s.adjoint(adj)[0]
-        out[tag] = (sec.astype(np.float64), gr.astype(np.float64))
-    ref_s, ref_g = out["fp64"]
-    res = {"run": f"workload grid, NT={nt}, against fp64 arithmetic with fp64 snapshots"}
-    for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s"):
-        s_, g_ = out[tag]
-        res[tag] = {"seismogram_rel_l2": _rel(s_[:2], ref_s[:2]), "gradient_rel_l2": _rel(g_[3:6], ref_g[3:6]),
-                    "misfit_rel": abs(float(np.sum(s_[:2] ** 2)) - float(np.sum(ref_s[:2] ** 2))) /
-                    float(np.sum(ref_s[:2] ** 2))}
+            l2, _ = s.residual_adjoint(obs, 1)
+            gr = s.adjoint(None, 1)[0]
+        out[tag] = (sec.astype(np.float64), gr.astype(np.float64), float(l2[0]))
+    ref_s, ref_g, ref_m = out["fp64"]
+    planes = [3, 4, 5] if q.wavetype != 2 else [8, 9]      # assembled per-shot gradients
+    raw = [0, 1, 2] if q.wavetype != 2 else [6, 7]         # the correlation sums before assembly
+    comps = [0, 1] if q.wavetype != 2 else [2]
+    res = {"run": f"one shot, NT={q.nt}, against fp64 arithmetic with fp64 snapshots; gradient = the assembled "
+                  f"{'vp, vs, rho' if q.wavetype != 2 else 'vs_z, rho_z'} planes (raw: the "
+                  f"{'lambda, mu, rho' if q.wavetype != 2 else 'mu_z, rho_z'} correlation sums), seismograms = "
+                  f"{'vx, vy' if q.wavetype != 2 else 'vz'}, misfit = FP64 L2 of the residual"}
+    for tag in formats:
+        s_, g_, m_ = out[tag]
+        res[tag] = {"seismogram_rel_l2": _rel(s_[comps], ref_s[comps]), "gradient_rel_l2": _rel(g_[planes], ref_g[planes]),
+                    "raw_gradient_rel_l2": _rel(g_[raw], ref_g[raw]),
+                    "misfit_rel": abs(m_ - ref_m) / max(abs(ref_m), 1e-300)}
     return res
 
 
@@ -326,10 +349,12 @@ def _timed_shots(solver, stream, nshots, run):
     return ev0.elapsed_time(ev1)
 
 
-def plain_path(p, models, shots, device, count=2, warmup=1):
+def plain_path(p, models, shots, device, count=2, warmup=1, roofline=False):
     """The drop-in path as the reference driver would use it: one shot per
     context, fp32 snapshots, every kernel launched step by step (no graph
-    replay, default options).  Returns shot-gradients/s."""
+    replay, default options).  Returns shot-gradients/s; with `roofline` (the
+    viscoelastic workload) also the sampled single-shot stress and velocity
+    launch times against their algorithmic bytes."""
     import torch
     from ifos_b200 import workloads as W
     from ifos_b200.solver import ShotSolver
@@ -357,10 +382,26 @@ def plain_path(p, models, shots, device, count=2, warmup=1):
             for k in range(count):
                 shot(warmup + k)
 
+        if roofline:
+            s.kernel_timing(8)
+            s.kernel_times(reset=True)
         ms = _timed_shots(s, stream, count, run)
+        kt = s.kernel_times(reset=True) if roofline else None
+        s.kernel_timing(0)
         s.set_stream(None)
-    return {"value": count / (ms / 1e3), "unit": METRIC, "shots": count, "ms_per_shot": ms / count,
-            "form": "1 shot per context, fp32 snapshots, step-by-step launches"}
+    out = {"value": count / (ms / 1e3), "unit": METRIC, "shots": count, "ms_per_shot": ms / count,
+           "form": "1 shot per context, fp32 snapshots, step-by-step launches"}
+    if kt:
+        peak, _ = measured_peak()
+        (s_ms, s_n), (v_ms, v_n) = kt["stress"], kt["velocity"]
+        b_s = stress_bytes(p, 1)
+        b_v = (velocity_bytes(p, False) + velocity_bytes(p, True)) / 2
+        out["kernels"] = {
+            "stress": {"avg_launch_ms": s_ms / max(1, s_n), "alg_bytes": b_s,
+                       "frac": b_s / (s_ms / max(1, s_n) / 1e3) / 1e9 / peak if s_n else None},
+            "velocity": {"avg_launch_ms": v_ms / max(1, v_n), "alg_bytes": b_v,
+                         "frac": b_v / (v_ms / max(1, v_n) / 1e3) / 1e9 / peak if v_n else None}}
+    return out
 
 
 def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
@@ -418,10 +459,13 @@ def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
         ms = _timed_shots(s, stream, len(shots), run)
         s.set_stream(None)
     value = len(shots) / (ms / 1e3)
+    mi, g0 = shots[0]
+    err = fp64_error(p, models[mi], g0, formats=("fp32", snap), device=device)
     physics = "plain-elastic" if wavetype == 1 else "SH elastic"
     return {"workload": f"batched {physics} 400x160 FDORDER{fdorder} NT2000 DTINV2, 256 shots over 5 models",
             "value": value, "unit": METRIC, "batch": B, "snapshots": snap, "options": choice["options"],
-            "ms_all_shots": ms, "plain_fp32": plain, "speedup_vs_plain_fp32": value / plain["value"]}
+            "ms_all_shots": ms, "plain_fp32": plain, "speedup_vs_plain_fp32": value / plain["value"],
+            "fp64_error": err}
 
 
 def serving_bench(device, snap, full=False, n_requests=32, loads=(0.5, 1.0, 1.5)):
@@ -564,7 +608,8 @@ def main():
     # ---- the plain FP32 path (drop-in form), for the speed-up of the batched form ----
     plain = None
     if not args.no_plain:
-        plain = plain_path(p, [model], [(0, geoms[shot_index(k, rank, world, len(geoms))]) for k in range(3)], device)
+        plain = plain_path(p, [model], [(0, geoms[shot_index(k, rank, world, len(geoms))]) for k in range(3)], device,
+                           roofline=True)
 
     # ---- the batched, low-precision-snapshot form: batch size and options tuned ----
     if args.batch > 0:
@@ -672,6 +717,34 @@ def main():
             b.close()
     solver.close()
 
+    # ---- the same batching and graphs with fp32 snapshots: the gain of the low-precision snapshots alone ----
+    batched_fp32 = None
+    if args.snap != "fp32" and not args.no_plain and world == 1:
+        free = torch.cuda.mem_get_info(device)[0]
+        Bf = B
+        while Bf > 1 and ShotSolver.bytes_needed(p, snapshots=True, max_shots=Bf, snap_format="fp32") > free * 0.85:
+            Bf -= 1
+        with ShotSolver(p, max_shots=Bf, max_rec=ntr, snap_format="fp32", device=device) as sf:
+            sf.set_options(**opts)
+            sf.upload_model(model)
+            sf.set_stream(stream.cuda_stream)
+            sf.stage_adjoint(adj_host[:Bf], Bf)
+
+            def step32(k):
+                for b in range(Bf):
+                    g, sig = shot(k * Bf + b)
+                    sf.setup_shot(b, g.srcpos, sig, g.recpos)
+                sf.forward(Bf, store=True, fetch=False)
+                sf.adjoint(None, Bf, fetch=False)
+
+            step32(0)
+            n32 = 2
+            ms32 = _timed_shots(sf, stream, n32 * Bf, lambda: [step32(1 + k) for k in range(n32)])
+            sf.set_stream(None)
+        batched_fp32 = {"value": n32 * Bf / (ms32 / 1e3), "unit": METRIC, "batch": Bf, "options": opts,
+                        "form": f"{Bf} shots per context (the most that fit), fp32 snapshots, graphs and the "
+                                "same options", "steps": n32}
+
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -682,24 +755,36 @@ def main():
     s_ms, s_n = ktimes["stress"]
     v_ms, v_n = ktimes["velocity"]
     avg_s = s_ms / max(1, s_n)
-    b_s = stress_bytes(p) * B  # one launch steps all B slots
+    avg_v = v_ms / max(1, v_n)
+    b_s = stress_bytes(p, B, models=1)  # one launch steps all B slots of the one model
+    b_s_ps = stress_bytes(p, B, per_shot_model=True)
     achieved = b_s / (avg_s / 1000.0) / 1e9 if s_n else None
+    achieved_ps = b_s_ps / (avg_s / 1000.0) / 1e9 if s_n else None
     tr = ncu_traffic(B)
     traffic = tr[0] * cells / tr[1] if tr else None
+    b_v = (velocity_bytes(p, False, B) + velocity_bytes(p, True, B)) / 2  # forward and adjoint launches alternate
     roof = {"kernel": f"viscoelastic stress update (L=3 memory variables + CPML), fp32, {B} shot(s) per launch",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None,
+            "accounting": "model coefficient planes counted once per launch (one model, read once for all "
+                          "slots); state per shot",
+            "frac_per_shot_accounting": achieved_ps / peak if achieved_ps else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
             "fallback 6650 GB/s",
-            "traffic": traffic, "traffic_source": (tr[2] + ", scaled to this grid by cells") if tr else None,
-            "alg_bytes_per_launch": b_s, "avg_launch_ms": avg_s, "sampled_launches": s_n,
-            "velocity_kernel": {"avg_launch_ms": v_ms / max(1, v_n),
-                                "achieved_gbs": B * (velocity_bytes(p, False) + velocity_bytes(p, True)) / 2 /
-                                (v_ms / max(1, v_n) / 1000.0) / 1e9 if v_n else None}}
+            "traffic": traffic,
+            "traffic_source": tr[2] if tr else f"no ncu capture of this build ({library_stamp()}) in "
+                                                "profiles/ncu_traffic.txt",
+            "alg_bytes_per_launch": b_s, "alg_bytes_per_launch_per_shot_accounting": b_s_ps,
+            "avg_launch_ms": avg_s, "sampled_launches": s_n,
+            "velocity_kernel": {"avg_launch_ms": avg_v, "alg_bytes_per_launch": b_v,
+                                "achieved_gbs": b_v / (avg_v / 1000.0) / 1e9 if v_n else None,
+                                "frac": b_v / (avg_v / 1000.0) / 1e9 / peak if v_n else None}}
+    if plain and plain.get("kernels"):
+        roof["plain_1shot"] = plain["kernels"]
     extra = {}
     if not args.no_error:
         try:
-            extra["fp64_error"] = fp64_error(p, model, geoms[0])
+            extra["fp64_error"] = fp64_error(p, model, geoms[0], formats=("fp32", args.snap), device=device)
         except Exception as exc:  # report, never hide
             extra["fp64_error"] = {"error": repr(exc)}
     if world == 1:
@@ -735,6 +820,8 @@ def main():
                        "per": f"step of {B} shot-gradient(s) (forward + adjoint)"},
         "plain_fp32": plain,
         "speedup_vs_plain_fp32": value / plain["value"] if plain else None,
+        "batched_fp32_snapshots": batched_fp32,
+        "speedup_vs_batched_fp32_snapshots": value / batched_fp32["value"] if batched_fp32 else None,
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
