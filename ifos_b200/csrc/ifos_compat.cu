@@ -841,16 +841,19 @@ void check_launch(const char *what) {
     if (e != cudaSuccess) die(what, e);
 }
 
-// sources of update_v_PML / update_v_acoustic_PML / update_v_PML_SH at sample nt
-std::vector<SrcI> gather_src(float **srcpos_loc, float **signals, float **signals1, int nsrc, int nt) {
+// sources of update_v_PML / update_v_acoustic_PML / update_v_PML_SH at sample nt.
+// Only the forward (sw 0) reads the azimuth and type rows 7 and 8: the
+// adjoint's sources are the receivers, a matrix(1,6,...) of positions only
+// (src/IFOS2D.c:2183), as src/update_v_PML.c:552-578 reads them.
+std::vector<SrcI> gather_src(float **srcpos_loc, float **signals, float **signals1, int nsrc, int nt, int sw) {
     std::vector<SrcI> v;
     for (int l = 1; l <= nsrc; l++) {
         SrcI q{};
         q.i = (int)srcpos_loc[1][l];
         q.j = (int)srcpos_loc[2][l];
-        q.type = (int)srcpos_loc[8][l];
+        q.type = sw == 0 ? (int)srcpos_loc[8][l] : 0;
         // azi_rad = srcpos_loc[7][l]*PI/180, a float, then sin/cos of it (src/update_v_PML.c:556,562)
-        const float azi = (float)(srcpos_loc[7][l] * kPi / 180);
+        const float azi = sw == 0 ? (float)(srcpos_loc[7][l] * kPi / 180) : 0.0f;
         q.sn = std::sin((double)azi);
         q.cs = std::cos((double)azi);
         q.s = signals ? signals[l][nt] : 0.0f;
@@ -897,7 +900,7 @@ extern "C" void update_v_PML(int nx1, int nx2, int ny1, int ny2, int nt, float *
         check_launch("update_v_PML");
     }
     if (nsrc > 0 && (sw == 0 || sw == 1)) {
-        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt);
+        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt, sw);
         const SrcI *d_src = (const SrcI *)small_up(src.data(), src.size() * sizeof(SrcI));
         kc_src_v<<<1, 1, 0, stream()>>>(g, d_src, nsrc, d_vx, d_vy, nullptr, d_rip, d_rjp, sw, ADJOINT_TYPE);
         check_launch("update_v_PML sources");
@@ -952,7 +955,7 @@ extern "C" void update_v_acoustic_PML(int nx1, int nx2, int ny1, int ny2, int nt
         check_launch("update_v_acoustic_PML");
     }
     if (nsrc > 0 && (sw == 0 || sw == 1)) {
-        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt);
+        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt, sw);
         const SrcI *d_src = (const SrcI *)small_up(src.data(), src.size() * sizeof(SrcI));
         kc_src_v<<<1, 1, 0, stream()>>>(g, d_src, nsrc, d_vx, d_vy, nullptr, d_rip, d_rjp, sw, ADJOINT_TYPE);
         check_launch("update_v_acoustic_PML sources");
@@ -1340,7 +1343,7 @@ extern "C" void update_v_PML_SH(int nx1, int nx2, int ny1, int ny2, int nt, floa
         check_launch("update_v_PML_SH");
     }
     if (nsrc > 0 && (sw == 0 || sw == 1)) {
-        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt);
+        const std::vector<SrcI> src = gather_src(srcpos_loc, signals, signals1, nsrc, nt, sw);
         const SrcI *d_src = (const SrcI *)small_up(src.data(), src.size() * sizeof(SrcI));
         kc_src_v<<<1, 1, 0, stream()>>>(g, d_src, nsrc, nullptr, nullptr, d_vz, nullptr, d_rjp, sw, ADJOINT_TYPE);
         check_launch("update_v_PML_SH sources");
