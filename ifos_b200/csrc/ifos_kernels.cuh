@@ -648,7 +648,24 @@ struct KRec {
     int max_rec;
     const float *adj;    // slot * 3 * max_rec * NT
     float *sec;          // slot * NS * max_rec * NT
+    // the cell -> receiver map the velocity ops use to sample or inject the
+    // receivers in place: per slot map_stride ints, first NY row entries
+    // (-1: no receiver in the row, else the row's index among the slot's
+    // receiver rows), then rmax rows of NX cell entries (-1 or the index of
+    // the receiver in the cell)
+    const int *map;
+    long long map_stride;
+    int rmax;
 };
+
+// receiver indices of cells (j, i) and (j, i+1) of `slot` (-1: none)
+__device__ __forceinline__ int2 rec_pair(const KRec &r, int nx, int ny, int slot, int j, int i, bool v0, bool v1) {
+    const int *m = r.map + (long long)slot * r.map_stride;
+    const int rr = m[j - 1];
+    if (rr < 0) return make_int2(-1, -1);
+    const int *cells = m + ny + (long long)rr * nx + (i - 1);
+    return make_int2(v0 ? cells[0] : -1, v1 ? cells[1] : -1);
+}
 
 template <typename T>
 __global__ void k_inject_v_fwd(KGrid g, KState<T> S, KModel<T> M, KSrc src, int nt, int psv, int sh) {

@@ -74,6 +74,10 @@ inline void launch_dep(cudaStream_t st, bool pdl, void (*kern)(KArgs...), dim3 g
 // largest L on the pipelined path (more SLS fall back to one thread per cell)
 static constexpr int kPipeMaxL = 5;
 
+// receiver rows a slot's cell map holds: slots whose receivers lie on more
+// rows are sampled and injected by the separate receiver kernels
+constexpr int kRecMapRows = 8;
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -106,8 +110,8 @@ struct ifos_ctx {
     KGrid g{};
     int psv = 0, sh = 0, ac = 0;
     // state
-    DevBuf state, psi, models, prof, srf, slot_model, src_pos, src_sig, src_n, rec_pos, rec_n, adj, sec, snap,
-        snap_scale, gacc, gout, bad, dot_partial, dot_out, res_tr;
+    DevBuf state, psi, models, prof, srf, slot_model, src_pos, src_sig, src_n, rec_pos, rec_n, rec_map, adj, sec,
+        snap, snap_scale, gacc, gout, bad, dot_partial, dot_out, res_tr;
     long long slot_stride = 0, psix_len = 0, psiy_len = 0, psi_slot = 0, model_stride = 0;
     long long off[NP_FIELD];
     long long mem_off[5];
@@ -123,6 +127,8 @@ struct ifos_ctx {
     int fwd_nshots = 0;
     // host mirrors
     std::vector<int> nsrc_h, ntr_h, slot_model_h;
+    std::vector<int> rec_row_lo, rec_row_hi;  // per slot: rows holding its receivers (lo > hi: none)
+    std::vector<char> rec_mapped;             // per slot: its receivers fit the cell map (kRecMapRows rows)
     std::vector<float> srcpos_h;
     bool adj_staged = false;
     float last_ms = 0.0f;
@@ -203,6 +209,9 @@ inline KRec krec(const ifos_ctx *c) {
     r.max_rec = std::max(1, c->p.max_rec);
     r.adj = (const float *)c->adj.p;
     r.sec = (float *)c->sec.p;
+    r.map = (const int *)c->rec_map.p;
+    r.map_stride = (long long)c->p.ny + (long long)kRecMapRows * c->p.nx;
+    r.rmax = kRecMapRows;
     return r;
 }
 inline KSnap ksnap(const ifos_ctx *c) {
@@ -246,6 +255,24 @@ struct Launcher {
     // (fsurf) of step nt_cur themselves: P-SV elastic and viscoelastic only
     int nt_cur = 0, fsurf = 0, fps = 0;
     int src_j0 = 1, src_j1 = 0;  // rows holding the slots' sources (empty range: none)
+    // the P-SV velocity ops sample (1) or inject (2) the receivers of rows
+    // rec_j0..rec_j1 themselves (the setting of the step being launched)
+    int rec_mode = 0, rec_j0 = 1, rec_j1 = 0;
+    bool seis_fused = false;  // the forward's velocity ops sample the receivers (no seismogram kernel)
+    // rows holding the receivers of slots [0, nshots); false when a slot's
+    // receivers do not fit its cell map
+    bool receiver_rows() {
+        rec_j0 = c->p.ny + 1;
+        rec_j1 = 0;
+        bool ok = true;
+        for (int s = 0; s < nshots; s++) {
+            if (c->ntr_h[s] <= 0) continue;
+            ok = ok && c->rec_mapped[s];
+            rec_j0 = std::min(rec_j0, c->rec_row_lo[s]);
+            rec_j1 = std::max(rec_j1, c->rec_row_hi[s]);
+        }
+        return ok;
+    }
     Launcher(ifos_ctx *cc, int ns) : c(cc), nshots(ns) {
         S = kstate<T>(c);
         M = kmodel<T>(c);
@@ -255,8 +282,15 @@ struct Launcher {
     }
     // one persistent launch of a pipelined stencil op over all tiles of all slots
     template <typename Op>
-    void pipelined(const Op &op) {
+    void pipelined(const Op &op0) {
         using P = typename Op::P;
+        Op op = op0;
+        op.nt = nt_cur;
+        op.rec = rec;
+        op.rec_mode = rec_mode;
+        op.rec_j0 = rec_j0;
+        op.rec_j1 = rec_j1;
+        op.bad = (int *)c->bad.p;
         static_assert(P::bytes() + 1024 <= 232448, "shared-memory ring exceeds 227 KB");
         auto kern = kp_stencil<Op>;
         constexpr int kMaxDev = 64;
@@ -442,6 +476,7 @@ struct Launcher {
                                              c->psv, c->sh, c->ac, psource ? 1 : 0, c->p.free_surf ? 1 : 0, pt));
             c->launches++;
         }
+        if (seis_fused) return;  // the velocity op sampled the receivers and probed for NaN
         const dim3 gr((unsigned)((std::max(1, c->p.max_rec) + 127) / 128), (unsigned)nshots);
         DISPATCH_FDOH(g.fdoh, launch_dep(c->st, c->pdl, k_seismo<T, FD>, gr, dim3(128), 0, g, S, M, rec, nt,
                                          c->p.seismo, c->psv, c->sh, c->ac, (int *)c->bad.p));

@@ -217,8 +217,8 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->cp_st) cudaStreamSynchronize(c->cp_st);  // asynchronous fetches still reading the buffers
     DevBuf *bufs[] = {&c->state, &c->psi, &c->models, &c->prof, &c->srf, &c->slot_model, &c->src_pos, &c->src_sig,
-                      &c->src_n, &c->rec_pos, &c->rec_n, &c->adj, &c->sec, &c->snap, &c->snap_scale, &c->gacc,
-                      &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
+                      &c->src_n, &c->rec_pos, &c->rec_n, &c->rec_map, &c->adj, &c->sec, &c->snap, &c->snap_scale,
+                      &c->gacc, &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
     for (DevBuf *b : bufs) dev_free(*b);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     drop_graph(c->gfwd);
@@ -442,6 +442,10 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     if ((rc = dev_alloc(c, c->src_n, (size_t)S * sizeof(int)))) return bail(rc);
     if ((rc = dev_alloc(c, c->rec_pos, (size_t)S * 2 * mr * 4))) return bail(rc);
     if ((rc = dev_alloc(c, c->rec_n, (size_t)S * sizeof(int)))) return bail(rc);
+    if ((rc = dev_alloc(c, c->rec_map, (size_t)S * ((size_t)p.ny + (size_t)kRecMapRows * p.nx) * sizeof(int))))
+        return bail(rc);
+    if (cudaMemsetAsync(c->rec_map.p, 0xff, c->rec_map.bytes, c->st) != cudaSuccess)  // -1: no receiver
+        return bail(fail(c, IFOS_ERR_CUDA, "receiver map clear failed"));
     if ((rc = dev_alloc(c, c->adj, (size_t)S * 3 * mr * p.nt * 4))) return bail(rc);
     if ((rc = dev_alloc(c, c->sec, (size_t)S * IFOS_NS * mr * p.nt * 4))) return bail(rc);
     const long long N = (long long)p.nx * p.ny;
@@ -508,6 +512,9 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     }
     c->nsrc_h.assign(S, 0);
     c->ntr_h.assign(S, 0);
+    c->rec_row_lo.assign(S, 1);
+    c->rec_row_hi.assign(S, 0);
+    c->rec_mapped.assign(S, 1);
     c->slot_model_h.assign(S, 0);
     c->srcpos_h.assign((size_t)S * 8 * ms, 0.0f);
     setup_pipeline(c, L);
@@ -637,6 +644,29 @@ extern "C" int ifos_shot_setup(ifos_ctx *c, int slot, int model, int nsrc, const
                            cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync((char *)c->rec_pos.p + (size_t)slot * 2 * mr * 4, rp.data(), rp.size() * 4,
                        cudaMemcpyHostToDevice, c->st));
+    // the slot's cell -> receiver map for the in-stencil sampling and injection
+    const size_t mstride = (size_t)p.ny + (size_t)kRecMapRows * p.nx;
+    std::vector<int> rm(mstride, -1);
+    int lo = p.ny + 1, hi = 0, nrows = 0;
+    bool mapped = true;
+    for (int l = 0; l < ntr; l++) {
+        const int i = recpos[l], j = recpos[ntr + l];
+        lo = std::min(lo, j);
+        hi = std::max(hi, j);
+        if (rm[j - 1] < 0) {
+            if (nrows == kRecMapRows) {
+                mapped = false;
+                continue;
+            }
+            rm[j - 1] = nrows++;
+        }
+        rm[(size_t)p.ny + (size_t)rm[j - 1] * p.nx + (i - 1)] = l;
+    }
+    CK(cudaMemcpyAsync((char *)c->rec_map.p + (size_t)slot * mstride * 4, rm.data(), rm.size() * 4,
+                       cudaMemcpyHostToDevice, c->st));
+    c->rec_mapped[slot] = mapped;
+    c->rec_row_lo[slot] = lo;
+    c->rec_row_hi[slot] = hi;
     c->nsrc_h[slot] = nsrc;
     c->ntr_h[slot] = ntr;
     c->slot_model_h[slot] = model;
@@ -760,6 +790,11 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     const bool in_stress = c->pipe && c->psv && !c->ac && !c->sh;
     Lr.fps = in_stress ? 1 : 0;
     Lr.fsurf = (in_stress && p.free_surf) ? 1 : 0;
+    // P-SV without force sources, SEISMO 1: vx, vy are final when the velocity
+    // op stores them, so it samples the receivers itself (and probes for NaN)
+    const bool rec_ok = Lr.receiver_rows();
+    const bool seis_fused = std::is_same<T, float>::value && in_stress && !force && p.seismo == 1 && rec_ok;
+    Lr.seis_fused = seis_fused;
     {
         const int ms = std::max(1, p.max_src);
         int lo = p.ny + 1, hi = 0;
@@ -797,7 +832,9 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
         Lr.nt_cur = nt;
         {
             KTimer t(c, 0, sample);
+            Lr.rec_mode = seis_fused ? 1 : 0;
             Lr.v_step(0, snap_now ? 1 : 0, fhin);
+            Lr.rec_mode = 0;
         }
         if (force) {
             launch_dep(c->st, c->pdl, k_inject_v_fwd<T>, dim3(nshots), dim3(32), 0, c->g, Lr.S, Lr.M, Lr.src, nt, c->psv && !c->ac ? 1 : (c->ac ? 1 : 0),
@@ -836,7 +873,8 @@ static int forward_t(ifos_ctx *c, int nshots, int store, int nsteps) {
     }
     };
     // the source rows are launch parameters of the stress kernels: part of the captured sequence
-    if (int rc = run_loop(c, c->gfwd, loop_key(c, {0, nshots, snaps, nsteps, force, fused, Lr.src_j0, Lr.src_j1}),
+    if (int rc = run_loop(c, c->gfwd, loop_key(c, {0, nshots, snaps, nsteps, force, fused, Lr.src_j0, Lr.src_j1,
+                                                    seis_fused, Lr.rec_j0, Lr.rec_j1}),
                           enqueue))
         return rc;
     CK(cudaEventRecord(c->ev1, c->st));
@@ -869,26 +907,35 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     const int ntd = p.nt / p.dtinv;
     const int mr = std::max(1, p.max_rec);
     dim3 gr_rec((mr + 127) / 128, nshots);
+    // P-SV (elastic or viscoelastic) on the pipelined path: the velocity op
+    // adds the residual sources itself
+    const bool rec_ok = Lr.receiver_rows();
+    const bool inj_fused = std::is_same<T, float>::value && c->pipe && c->psv && !c->ac && !c->sh &&
+                           p.adjoint_type >= 1 && p.adjoint_type <= 3 && rec_ok;
     CK(cudaEventRecord(c->ev0, c->st));
     auto enqueue = [&]() {
     int hin_a = 1;
     for (int nt = 1; nt <= p.nt; nt++) {
         const bool sample = c->prof_stride > 0 && (nt % c->prof_stride) == 0;
+        Lr.nt_cur = nt;
         {
             KTimer t(c, 0, sample);
+            Lr.rec_mode = inj_fused ? 2 : 0;
             Lr.v_step(1, 0);
+            Lr.rec_mode = 0;
         }
-        if ((c->psv && p.adjoint_type >= 1 && p.adjoint_type <= 3) || c->sh) {
+        if (!inj_fused && ((c->psv && p.adjoint_type >= 1 && p.adjoint_type <= 3) || c->sh)) {
             launch_dep(c->st, c->pdl, k_inject_v_adj<T>, dim3(gr_rec), dim3(128), 0, c->g, Lr.S, Lr.rec, nt, c->psv ? 1 : 0, c->sh && !c->ac);
             c->launches++;
         }
+        const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
+        const bool snap_step = (fstep - 1) % p.dtinv == 0;
         {
             KTimer t(c, 1, sample);
             Lr.s_step();
         }
         Lr.post_adj(nt, p.adjoint_type == 4);
-        const int fstep = p.nt - nt + 1;  // forward step this adjoint step meets
-        if ((fstep - 1) % p.dtinv == 0) {
+        if (snap_step) {
             KTimer t(c, 3, sample);
             bool pairs = false;
             if constexpr (std::is_same<T, float>::value) {
@@ -928,7 +975,8 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     launch_dep(c->st, c->pdl, k_assemble<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.M, gr, c->psv, c->sh, c->ac);
     c->launches++;
     };
-    if (int rc = run_loop(c, c->gadj, loop_key(c, {1, nshots}), enqueue)) return rc;
+    if (int rc = run_loop(c, c->gadj, loop_key(c, {1, nshots, inj_fused, Lr.rec_j0, Lr.rec_j1}), enqueue))
+        return rc;
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev1));

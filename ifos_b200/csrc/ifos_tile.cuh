@@ -23,6 +23,7 @@
 #include <type_traits>
 
 #include "ifos_kernels.cuh"
+#include "ifos_snap.cuh"
 #include "ifos_tma.cuh"
 
 // 1: the reference's double-promoted terms are evaluated in double (bit-exact);
@@ -537,6 +538,43 @@ static __device__ __noinline__ float4 psource_row_v(const KGrid &g, const KSrc &
     psource_row(g, src, slot, nt, j, cl, sxx, syy);
     return make_float4(sxx[0], sxx[1], syy[0], syy[1]);
 }
+// Receiver indices of the thread's column pair in row j (-1: none) when
+// the velocity op samples or injects the receivers in place (rec_mode), read
+// from the slot's cell map at the start of the row so that the two loads are
+// in flight while the row is computed.
+__device__ __forceinline__ int2 rec_lookup(const KGrid &g, const KRec &rec, int mode, int rec_j0, int rec_j1,
+                                           int slot, int j, const Cols &cl) {
+    if (!mode || j < rec_j0 || j > rec_j1 || j > g.ny) return make_int2(-1, -1);
+    return rec_pair(rec, g.nx, g.ny, slot, j, cl.i, cl.v0, cl.v1);
+}
+
+// The receivers of the thread's cells in row j (rl: their indices) on the
+// new vx, vy before they are stored: mode 1 copies them into the seismograms
+// of step nt, as src/seismo_ssg.c:26-140 samples vx, vy after the step
+// (SEISMO 1); mode 2 adds the adjoint sources of step nt, as
+// src/update_v_PML.c:567-578 does after the velocity update (ADJOINT_TYPE 1:
+// both components, 2: vy, 3: vx).
+__device__ __forceinline__ void rec_apply(const KGrid &g, const KRec &rec, int mode, int slot, int nt, int2 rl,
+                                          float (&vx)[2], float (&vy)[2]) {
+    const long long cs = (long long)rec.max_rec * g.nt_total;
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+        const int l = e ? rl.y : rl.x;
+        if (l < 0) continue;
+        const long long o = (long long)l * g.nt_total + nt - 1;
+        if (mode == 2) {
+            const float *adj = rec.adj + (long long)slot * 3 * cs + o;
+            const int at = g.adjoint_type;
+            if (at == 1 || at == 3) vx[e] += adj[0];
+            if (at == 1 || at == 2) vy[e] += adj[cs];
+        } else {
+            float *sec = rec.sec + (long long)slot * 6 * cs + o;
+            sec[0] = vx[e];
+            sec[cs] = vy[e];
+        }
+    }
+}
+
 template <int FDOH, int HE, int LL>
 __device__ __noinline__ RowVals<LL> surface_row_v(const KGrid &g, const KState<float> &S, const KModel<float> &M,
                                                   Hc<FDOH> hc, XWin<HE> wx, float2 vy2, Cols cl, int slot, int model,
@@ -563,6 +601,10 @@ __device__ __noinline__ RowVals<LL> surface_row_v(const KGrid &g, const KState<f
 // src, nt, fsurf, fps: the stress ops apply the explosive sources of step nt
 // (fps; rows src_j0..src_j1 hold every slot's sources) and the free surface
 // of row 1 (fsurf) themselves
+// rec_mode (P-SV velocity ops): 1 the forward samples vx, vy at the
+// receivers into the seismograms (SEISMO 1) and probes the centre cell for
+// NaN, 2 the adjoint adds the residual sources at the receivers; rows
+// rec_j0..rec_j1 hold every slot's receivers.
 #define IFOS_OP_MEMBERS \
     KGrid g;            \
     KState<float> S;    \
@@ -573,7 +615,11 @@ __device__ __noinline__ RowVals<LL> surface_row_v(const KGrid &g, const KState<f
     int nt;             \
     int fsurf;          \
     int fps;            \
-    int src_j0, src_j1;
+    int src_j0, src_j1; \
+    KRec rec;           \
+    int rec_mode;       \
+    int rec_j0, rec_j1; \
+    int *bad;
 
 // ---------------------------------------------------------------------------
 // stress, P-SV viscoelastic with LL SLS (src/update_s_visc_PML.c; the
@@ -897,6 +943,10 @@ struct OpVPsv {
         // P-SV: sxx, syy, sxy boxes; acoustic: the sp box serves as all three
         const float *t_sxx = h, *t_syy = AC ? h : h + P::BOXS, *t_sxy = AC ? h : h + 2 * P::BOXS;
         const Hc<FDOH> hc(g);
+        int2 rl[RT];  // receivers of the thread's cells (rec_mode)
+#pragma unroll
+        for (int r = 0; r < RT; r++)
+            rl[r] = rec_lookup(g, rec, rec_mode, rec_j0, rec_j1, ti.slot, ti.j0 + threadIdx.y * RT + r, cl);
         XWin<P::HE> wxx[RT], wxy[RT];
         float2 dyy[RT], dxy[RT], in[RT][NP_];
         float2 qa[RT][QUIRK && !AC ? FDOH : 1];  // reference 10/12 P-SV form: the sxy y-taps one by one
@@ -981,6 +1031,11 @@ struct OpVPsv {
                 }
                 o[0][e] = vxo + div_dh(g, DT * rip * fx);
                 o[1][e] = vyo + div_dh(g, DT * rjp * fy);
+            }
+            if (rl[r].x >= 0 || rl[r].y >= 0) rec_apply(g, rec, rec_mode, slot, nt, rl[r], o[0], o[1]);
+            if (rec_mode == 1 && j == g.ny / 2) {  // the instability probe of the driver (src/IFOS2D.c:1660-1672)
+                const int e = g.nx / 2 - cl.i;
+                if ((e == 0 || e == 1) && cl.valid(e) && isnan(e ? o[1][1] : o[1][0])) atomicExch(bad, 1);
             }
             const RowOut out(g, S, so, slot, j, cl);
             out.put(S.off[P_VX], o[0][0], o[0][1]);
