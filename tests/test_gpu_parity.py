@@ -34,6 +34,35 @@ def test_shot_matches_oracle(name):
     assert bit_equal(gpu["adj_fields"], ref["adj_fields"]), "adjoint fields not bit-identical"
 
 
+# receiver layouts of the in-place sampling and injection of the P-SV velocity op: receivers on a few rows
+# (the cell map), on more rows than the map holds (the separate receiver kernels), at the grid's centre cell
+# (the instability probe's cell), and the single-component adjoint sources (ADJOINT_TYPE 2 and 3)
+@pytest.mark.parametrize("layout,adjoint_type", [("three_rows", 1), ("three_rows", 2), ("three_rows", 3),
+                                                 ("vertical_line", 1), ("centre", 1)])
+@pytest.mark.parametrize("name", ["psv_el_o4", "psv_visc_o4"])
+def test_receiver_layouts_match_oracle(name, layout, adjoint_type):
+    p, model, g, sig, adj = build_case(name)
+    p.adjoint_type = adjoint_type
+    if layout == "three_rows":
+        xs = np.concatenate([np.arange(10, 55, 4), np.arange(12, 50, 5), np.arange(9, 57, 6)])
+        ys = np.concatenate([np.full(12, 3), np.full(8, 11), np.full(8, 20)])
+    elif layout == "vertical_line":
+        ys = np.arange(3, 36, 3)
+        xs = np.full(ys.shape, 30)
+    else:
+        xs, ys = np.array([p.nx // 2, 10, 50]), np.array([p.ny // 2, 3, 3])
+    rec = np.stack([xs, ys]).astype(np.int32)
+    g = W.Geometry(g.srcpos, rec)
+    rng = np.random.default_rng(5)
+    adj = (rng.standard_normal((3, rec.shape[1], p.nt)) * 1e-3).astype(np.float32)
+    gpu = gpu_shot(p, model, g, sig, adj)
+    ref = oracle_shot(p, model, g, sig, adj)
+    m = forward_fields_mask()
+    for key in ("sections", "grads", "adj_fields"):
+        assert bit_equal(gpu[key], ref[key]), key
+    assert bit_equal(gpu["fields"][m], ref["fields"][m]), "fields"
+
+
 @pytest.mark.parametrize("name,nx,ny,fw", [("psv_el_o4", 131, 37, 10), ("psv_visc_o8_holberg", 77, 29, 6),
                                             ("sh_visc_o4", 45, 23, 5), ("ac_visc_o2_nofs", 129, 41, 7),
                                             ("psv_el_o12_ref", 99, 51, 8), ("acoustic_o4_p", 65, 33, 4)])
