@@ -29,7 +29,7 @@ EXPORTS = [
     "ifos_taper_grad_shot", "ifos_median_smooth", "ifos_mat_change_test", "ifos_fetch_sections_async",
     "ifos_fetch_grads_async", "ifos_fetch_wait", "ifos_host_alloc", "ifos_host_free", "ifos_status",
 ]
-OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3}
+OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3, "wait_limit": 4}
 
 
 class IfosParams(C.Structure):

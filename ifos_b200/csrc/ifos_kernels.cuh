@@ -53,6 +53,7 @@ struct KGrid {
     int dh_pow2;     // DH is a power of two: x/DH == x*inv_dh exactly
     float inv_dh;    // 1/DH (exact when dh_pow2)
     int tile_order;  // pipelined stencils: 0 slot-major tile sequence, 1 slot-minor
+    int prod_polls;  // pipelined stencils: polls of the producer's stage-release wait (0: the default limit)
 };
 
 // x / DH, exact in both branches: multiplying by the reciprocal of a power of

@@ -761,7 +761,7 @@ static std::string loop_key(const ifos_ctx *c, std::initializer_list<long long> 
     std::string k;
     for (long long x : v) k += std::to_string(x) + ",";
     k += std::to_string(c->prof_stride) + "," + std::to_string(c->pdl) + "," + std::to_string(c->blocks_per_sm) + "," +
-         std::to_string(c->g.tile_order);
+         std::to_string(c->g.tile_order) + "," + std::to_string(c->g.prod_polls);
     return k;
 }
 
@@ -1819,6 +1819,10 @@ extern "C" int ifos_set_option(ifos_ctx *c, int option, int value) {
             if (value != 0 && value != 1) return fail(c, IFOS_ERR_ARG, "tile order must be 0 or 1");
             c->g.tile_order = value;
             break;
+        case IFOS_OPT_WAIT_LIMIT:
+            if (value < 0) return fail(c, IFOS_ERR_ARG, "the wait limit must be >= 0");
+            c->g.prod_polls = value;
+            break;
         default: return fail(c, IFOS_ERR_ARG, "unknown option " + std::to_string(option));
     }
     return IFOS_OK;
@@ -1831,6 +1835,7 @@ extern "C" int ifos_get_option(const ifos_ctx *c, int option, int *value) {
         case IFOS_OPT_PDL: *value = c->pdl ? 1 : 0; break;
         case IFOS_OPT_BLOCKS_PER_SM: *value = c->blocks_per_sm; break;
         case IFOS_OPT_TILE_ORDER: *value = c->g.tile_order; break;
+        case IFOS_OPT_WAIT_LIMIT: *value = c->g.prod_polls; break;
         default: return IFOS_ERR_ARG;
     }
     return IFOS_OK;

@@ -168,14 +168,17 @@ struct PlainSrc {
 // travel through shared memory with the stage.  Every wait is bounded: a
 // wait that gives up records its code in *err (16/17: a compute warp on a
 // stage's loads, 18: the producer on a stage's release) and the block winds
-// down after its copies in flight.
+// down after its copies in flight: when the producer gives up before tile
+// k_stop it records k_stop (stop_at) and issues nothing more; the compute
+// warps still wait for every tile it issued (so that no copy into the ring is
+// in flight when the block exits), compute none of them, and leave at k_stop.
 template <typename P, typename Op>
 __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, int nshots, const Op &op, int *err) {
     constexpr int NST = P::STAGES, NH = P::NHALO, NP = P::NLOAD, TY = P::TILE_Y;
     extern __shared__ __align__(1024) unsigned char sm_raw[];
     __shared__ __align__(8) uint64_t full[NST], empty[NST];
     __shared__ TileInfo tinfo[NST];
-    __shared__ int abort_flag;
+    __shared__ int stop_at;  // -1 while the producer runs, else the first tile it did not issue
     float *smem = reinterpret_cast<float *>(sm_raw);
     const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + TY - 1) / TY;
     const int ntiles = ntx * nty * nshots;
@@ -185,7 +188,7 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], kComputeWarps);
         }
-        abort_flag = 0;
+        stop_at = -1;
         fence_mbar_init();
     }
     __syncthreads();
@@ -233,24 +236,31 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
             const int t = blockIdx.x + k * gridDim.x;
             if (t >= ntiles) break;
             const int st = k % NST;
-            if (!mbar_wait_bounded(&empty[st], (uint32_t)(((k / NST) - 1) & 1), err, 18)) {
-                abort_flag = 1;
+            if (!mbar_wait_bounded(&empty[st], (uint32_t)(((k / NST) - 1) & 1), err, 18, (long)g.prod_polls)) {
+                *(volatile int *)&stop_at = k;
                 break;
             }
             issue(k, true, true);
         }
         return;
     }
+    volatile int *stop = &stop_at;
     for (int k = 0;; k++) {
         const int t = blockIdx.x + k * gridDim.x;
         if (t >= ntiles) break;
         const int st = k % NST;
         const uint32_t parity = (uint32_t)((k / NST) & 1);
-        if (!mbar_wait_bounded(&full[st], parity, err, 16)) {
+        bool landed = false;
+        for (long it = 0; it < (1L << 16) && !landed; it++) {
+            landed = mbar_try_wait(&full[st], parity);
+            if (!landed && *stop >= 0 && k >= *stop) return;  // never issued: nothing in flight for it
+        }
+        if (!landed) {
+            if (err) atomicExch(err, 16);
             mbar_wait_bounded(&full[st], parity, err, 17);
             return;
         }
-        if (abort_flag) return;
+        if (*stop >= 0) continue;  // the producer stopped: drain the tiles it issued, compute none
         const TileInfo ti = tinfo[st];
         const float *stage = smem + st * P::STAGE;
         op.compute(ti, stage, stage + NH * P::BOXS, &empty[st]);

@@ -47,6 +47,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+// Non-blocking test of a phase (no suspension).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // 3-D tiled bulk tensor load into shared memory, completion on `bar`.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
     asm volatile(
@@ -60,9 +73,17 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 // suspend hint, so about a second in all), records `code` in *err and returns
 // false.  The TMA engine cannot stall indefinitely on in-bounds loads, so the
 // limit is only a guard.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err, int code) {
-    for (long it = 0; it < (1L << 16); it++)
-        if (mbar_try_wait(bar, parity)) return true;
+// With an explicit `polls` (a caller-set limit) every poll is a
+// non-blocking test, so that a short limit runs out in a few instructions.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err, int code,
+                                                  long polls = 0) {
+    if (polls > 0) {
+        for (long it = 0; it < polls; it++)
+            if (mbar_test_wait(bar, parity)) return true;
+    } else {
+        for (long it = 0; it < (1L << 16); it++)
+            if (mbar_try_wait(bar, parity)) return true;
+    }
     if (err) atomicExch(err, code);
     return false;
 }

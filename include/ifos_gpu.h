@@ -268,9 +268,9 @@ int ifos_grad_sum_device(ifos_ctx *ctx, int nshots, float *dev_out);
 int ifos_set_stream(ifos_ctx *ctx, void *stream);
 
 /* Execution options of a context (no counterpart in the reference; they
- * change how the loops run, never what they compute: every setting gives
- * bit-identical results).  A change takes effect at the next loop and
- * discards the loops captured so far. */
+ * change how the loops run, never what they compute: every setting of the
+ * first four gives bit-identical results).  A change takes effect at the
+ * next loop and discards the loops captured so far. */
 enum {
     /* 1 (default): each time loop (ifos_forward, ifos_adjoint) is captured
      * once into a CUDA graph per launch sequence and replayed for every
@@ -284,7 +284,15 @@ enum {
     /* 0 (default): the stencil launches walk all tiles of slot 0, then of
      * slot 1, ...; 1: the same tile of consecutive slots on consecutive
      * CTAs, so that shots over one model share its coefficient tiles in L2. */
-    IFOS_OPT_TILE_ORDER = 3
+    IFOS_OPT_TILE_ORDER = 3,
+    /* polls of the pipelined stencils' stage-release wait (the producer
+     * waiting for the compute warps to free a ring stage); 0 (default): about
+     * a second.  A wait that runs out stops the launch: its block issues no
+     * more copies, waits for those in flight, and the loop returns
+     * IFOS_ERR_CUDA ("barrier wait timed out", also reported by ifos_status)
+     * with the context still usable.  A limit of a few polls makes that
+     * happen on purpose, to test the error path. */
+    IFOS_OPT_WAIT_LIMIT = 4
 };
 int ifos_set_option(ifos_ctx *ctx, int option, int value);
 int ifos_get_option(const ifos_ctx *ctx, int option, int *value);

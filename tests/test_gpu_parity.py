@@ -240,6 +240,34 @@ def test_fp16_segment_snapshots_agree_across_paths_and_batches(fmt):
     assert bit_equal(grads[1], a["grads"])
 
 
+def test_stage_release_wait_runs_out_cleanly():
+    """The bounded wait of the pipelined stencils made to run out: with
+    IFOS_OPT_WAIT_LIMIT = 1 the producer tests a ring stage once for release
+    and, finding it still in use, stops the launch.  The loop returns
+    IFOS_ERR_CUDA with the timeout message and ifos_status reports it; the
+    copies already issued are waited for before the blocks exit, so the same
+    context then runs the shot with the default limit, bit-identical to the
+    oracle, and so does a fresh one.  (A grid of 1200 x 300 on one block per
+    SM gives every block several tiles, so the ring wraps.)"""
+    from ifos_b200._lib import IfosError
+    p, model, g, sig, adj = build_case("psv_visc_o4", nx=1200, ny=300, nt=20)
+    ref = oracle_shot(p, model, g, sig, adj)
+    with ShotSolver(p, max_rec=g.recpos.shape[1], max_src=g.srcpos.shape[1]) as s:
+        s.set_options(wait_limit=1, blocks_per_sm=1, graphs=0)
+        s.upload_model(model)
+        s.setup_shot(0, g.srcpos, sig, g.recpos)
+        with pytest.raises(IfosError) as e:
+            s.forward(1, store=True)
+        assert e.value.code == 2 and "timed out" in str(e.value)
+        assert s.status() == 2
+        s.set_options(wait_limit=0)
+        sec = s.forward(1, store=True)[0]
+        grads = s.adjoint(adj[None])[0]
+    assert bit_equal(sec, ref["sections"]) and bit_equal(grads, ref["grads"])
+    fresh = gpu_shot(p, model, g, sig, adj)
+    assert bit_equal(fresh["sections"], ref["sections"]) and bit_equal(fresh["grads"], ref["grads"])
+
+
 def test_error_paths_return_status_not_fault():
     p, model, g, sig, adj = build_case("psv_el_o4")
     from ifos_b200._lib import IfosError

@@ -68,9 +68,9 @@ def test_options_keep_results_bit_identical():
 def test_option_values_checked_and_reported():
     p, *_ = build_case("psv_el_o4")
     with ShotSolver(p, snapshots=False) as s:
-        assert s.options() == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=0)
+        assert s.options() == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=0, wait_limit=0)
         s.set_options(tile_order=1, blocks_per_sm=2, graphs=0)
-        assert s.options() == dict(graphs=0, pdl=1, blocks_per_sm=2, tile_order=1)
+        assert s.options() == dict(graphs=0, pdl=1, blocks_per_sm=2, tile_order=1, wait_limit=0)
         with pytest.raises(Exception):
             s.set_options(tile_order=2)
         with pytest.raises(Exception):
