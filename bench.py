@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--serving-full", action="store_true", help="full-size serving stream (grids to 3000x1000)")
     ap.add_argument("--precision-nt", type=int, default=1200,
                     help="NT of the precision study (8000 is the precision workload's full NT)")
+    ap.add_argument("--precision-only", action="store_true",
+                    help="run only the precision study (at --precision-nt) and print its JSON")
     return ap.parse_args()
 
 
@@ -322,7 +324,9 @@ def precision_study(device, nt=1200):
         runs = {}
         for tag, kw in (("fp64", dict(precision="fp64")), ("fp32", {}), ("bf16", dict(snap_format="bf16")),
                         ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s")),
-                    ("i16s", dict(snap_format="i16s"))):
+                        ("i16s", dict(snap_format="i16s")),
+                        # the correlation sums in double: separates the accumulation from the propagation
+                        ("fp32_acc64", dict(grad_acc64=True)), ("i16s_acc64", dict(snap_format="i16s", grad_acc64=True))):
             with ShotSolver(p, max_rec=ntr, device=device, **kw) as s:
                 s.upload_model(model)
                 s.setup_shot(0, g.srcpos, sig, g.recpos)
@@ -333,7 +337,7 @@ def precision_study(device, nt=1200):
         rs, rg, rm = runs["fp64"]
         out[name] = {tag: {"seismogram_rel_l2": _rel(runs[tag][0], rs), "gradient_rel_l2": _rel(runs[tag][1], rg),
                            "misfit_rel": abs(runs[tag][2] - rm) / max(abs(rm), 1e-300)}
-                     for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s")}
+                     for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s", "fp32_acc64", "i16s_acc64")}
     return out
 
 
@@ -578,6 +582,9 @@ def main():
         return 0
 
     import torch
+    if args.precision_only:
+        print(json.dumps({"precision": precision_study(local, nt=args.precision_nt)}), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime

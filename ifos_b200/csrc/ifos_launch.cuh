@@ -111,7 +111,7 @@ struct ifos_ctx {
     int psv = 0, sh = 0, ac = 0;
     // state
     DevBuf state, psi, models, prof, srf, slot_model, src_pos, src_sig, src_n, rec_pos, rec_n, rec_map, adj, sec,
-        snap, snap_scale, gacc, gout, bad, dot_partial, dot_out, res_tr;
+        snap, snap_scale, gacc, gacc64, gout, bad, dot_partial, dot_out, res_tr;
     long long slot_stride = 0, psix_len = 0, psiy_len = 0, psi_slot = 0, model_stride = 0;
     long long off[NP_FIELD];
     long long mem_off[5];

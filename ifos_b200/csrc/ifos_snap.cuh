@@ -160,6 +160,7 @@ struct KGrad {
     float *acc;             // slot * 5 * n
     float *out;             // slot * 10 * n (IFOS_G_* planes)
     long long n;
+    double *acc64;          // slot * 5 * n: the sums in double (grad_acc64), else NULL
 };
 
 // zero-lag correlation with the stored forward wavefield (src/IFOS2D.c:2379-2419)
@@ -215,37 +216,42 @@ struct CorrCell {
     float vxp1, vyp1, sxx, syy, sxy, sp, vzp1, sxz, syz;  // adjoint state
     float f[8];                                           // stored forward components
 };
-template <int PSV, int SH, int AC>
-__device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, float ll, float rho, float u, float *w0,
-                                               float *w1, float *w2, float *w3, float *w4) {
+// W: the accumulator type -- float as the reference accumulates (each
+// step's term is formed in float and added in float, or in double and
+// rounded, exactly as src/IFOS2D.c:2379-2419 writes it), or double for the
+// grad_acc64 sums (the same terms added in double, rounded once at the end)
+template <int PSV, int SH, int AC, typename W = float>
+__device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, float ll, float rho, float u, W *w0,
+                                               W *w1, W *w2, W *w3, W *w4) {
     constexpr int KS = PSV ? (AC ? 3 : 5) : 0;  // first SH component
     if (PSV) {
         const float frx = a.f[0], fry = a.f[1];
-        *w2 += (float)((a.vxp1 * frx) + (a.vyp1 * fry));
+        *w2 += (W)(float)((a.vxp1 * frx) + (a.vyp1 * fry));
         if (!AC) {
             const float fx = a.f[2], fy = a.f[3], fu = a.f[4];
-            *w0 += (float)((fx + fy) * (a.sxx + a.syy));
+            *w0 += (W)(float)((fx + fy) * (a.sxx + a.syy));
             if (mm != 0.0f) {
                 const double t1 = (1.0 / (double)mm) * (double)(fu * a.sxy);
                 const double t2 = (.25 * (double)(fx + fy * (a.sxx + a.syy))) / (double)ll;
                 const double t3 = (.25 * (double)(fx - fy * (a.sxx - a.syy))) / (double)mm;
-                *w1 = (float)((double)*w1 + ((t1 + t2) + t3));
+                *w1 = (W)((double)*w1 + ((t1 + t2) + t3));
             }
         } else {
             const float fp = a.f[2];
-            *w0 += (float)((fp) * (a.sp));
+            *w0 += (W)(float)((fp) * (a.sp));
         }
     }
     if (SH) {
         const float frz = a.f[KS], fxz = a.f[KS + 1], fyz = a.f[KS + 2];
-        *w4 += (float)(a.vzp1 * frz);
+        *w4 += (W)(float)(a.vzp1 * frz);
         const float muss = rho * u * u;
-        *w3 = (float)((double)*w3 + (1.0 / (double)(muss * muss)) * (double)(fxz * a.sxz + fyz * a.syz));
+        *w3 = (W)((double)*w3 + (1.0 / (double)(muss * muss)) * (double)(fxz * a.sxz + fyz * a.syz));
     }
 }
 
-// SEG: 0 fp32 snapshots, 1 fp16 segments, 2 int16 segments
-template <int PSV, int SH, int AC, int SEG>
+// SEG: 0 fp32 snapshots, 1 fp16 segments, 2 int16 segments; ACC64: the sums
+// in double (gr.acc64)
+template <int PSV, int SH, int AC, int SEG, bool ACC64 = false>
 __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSnap sn, KGrad gr, int snap) {
     pdl_wait();
     pdl_launch();
@@ -313,12 +319,30 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
         rho = ld2(M.m[M_RHO] + mo);
         u = ld2(M.m[M_VS] + mo);
     }
+    const bool pair = i + 1 <= g.nx;
+    if constexpr (ACC64) {
+        double *acd = gr.acc64 + (long long)slot * 5 * n + q;
+        double2 w[5] = {};
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+            if (use[k]) w[k] = *reinterpret_cast<const double2 *>(acd + k * n);
+        correlate_cell<PSV, SH, AC, double>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x);
+        if (pair)
+            correlate_cell<PSV, SH, AC, double>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y,
+                                                &w[4].y);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            if (!use[k]) continue;
+            if (pair) *reinterpret_cast<double2 *>(acd + k * n) = w[k];
+            else acd[k * n] = w[k].x;
+        }
+        return;
+    }
     float2 w[5] = {};
 #pragma unroll
     for (int k = 0; k < 5; k++)
         if (use[k]) w[k] = ld2(acc + k * n);
     correlate_cell<PSV, SH, AC>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x);
-    const bool pair = i + 1 <= g.nx;
     if (pair) correlate_cell<PSV, SH, AC>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y, &w[4].y);
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -327,6 +351,17 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
         else acc[k * n] = w[k].x;
     }
 }
+
+#ifndef IFOS_PIPE_FD
+// the double correlation sums rounded once to the float accumulators the
+// assembly reads (grad_acc64)
+__global__ void k_acc_round(const double *acc64, float *acc, long long n) {
+    pdl_wait();
+    pdl_launch();
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        acc[k] = (float)acc64[k];
+}
+#endif
 
 // per-shot gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2477-2601)
 template <typename T>

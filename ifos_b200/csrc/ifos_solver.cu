@@ -106,6 +106,10 @@ static int check_params(const ifos_params &p, std::string &why) {
         return IFOS_ERR_ARG;
     };
     if (p.nx < 1 || p.ny < 1 || p.nt < 1) return bad("NX, NY and NT must be positive");
+    if (p.grad_acc64 && (p.precision != 0 || (p.nx & 1) ||
+                         (p.snap_format != IFOS_SNAP_F32 && p.snap_format != IFOS_SNAP_F16S &&
+                          p.snap_format != IFOS_SNAP_I16S)))
+        return bad("grad_acc64 needs fp32 arithmetic, an even NX and fp32 or 16-bit segment snapshots");
     if (p.fdorder < 2 || p.fdorder > 12 || (p.fdorder & 1)) return bad("FDORDER must be 2, 4, 6, 8, 10 or 12");
     if (p.maxrelerror < 0 || p.maxrelerror > 4) return bad("MAXRELERROR must be 0..4");
     if (p.fw < 0 || 2 * p.fw > p.nx || 2 * p.fw > p.ny) return bad("FW does not fit the grid");
@@ -218,7 +222,7 @@ extern "C" int ifos_ctx_destroy(ifos_ctx *c) {
     if (c->cp_st) cudaStreamSynchronize(c->cp_st);  // asynchronous fetches still reading the buffers
     DevBuf *bufs[] = {&c->state, &c->psi, &c->models, &c->prof, &c->srf, &c->slot_model, &c->src_pos, &c->src_sig,
                       &c->src_n, &c->rec_pos, &c->rec_n, &c->rec_map, &c->adj, &c->sec, &c->snap, &c->snap_scale,
-                      &c->gacc, &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
+                      &c->gacc, &c->gacc64, &c->gout, &c->bad, &c->dot_partial, &c->dot_out, &c->res_tr};
     for (DevBuf *b : bufs) dev_free(*b);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     drop_graph(c->gfwd);
@@ -450,6 +454,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     if ((rc = dev_alloc(c, c->sec, (size_t)S * IFOS_NS * mr * p.nt * 4))) return bail(rc);
     const long long N = (long long)p.nx * p.ny;
     if ((rc = dev_alloc(c, c->gacc, (size_t)S * 5 * N * 4))) return bail(rc);
+    if (p.grad_acc64 && (rc = dev_alloc(c, c->gacc64, (size_t)S * 5 * N * 8))) return bail(rc);
     if ((rc = dev_alloc(c, c->gout, (size_t)S * IFOS_NG * N * 4))) return bail(rc);
     if ((rc = dev_alloc(c, c->bad, sizeof(int)))) return bail(rc);
     if ((rc = dev_alloc(c, c->dot_partial, 1024 * sizeof(double)))) return bail(rc);
@@ -901,9 +906,10 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
     if (int rc = zero_state<T>(c, nshots)) return rc;
     const long long N = (long long)p.nx * p.ny;
     CK(cudaMemsetAsync(c->gacc.p, 0, (size_t)nshots * 5 * N * 4, c->st));
+    if (c->gacc64.p) CK(cudaMemsetAsync(c->gacc64.p, 0, (size_t)nshots * 5 * N * 8, c->st));
     CK(cudaMemsetAsync(c->bad.p, 0, 4, c->st));
     KSnap sn = ksnap(c);
-    KGrad gr{(float *)c->gacc.p, (float *)c->gout.p, N};
+    KGrad gr{(float *)c->gacc.p, (float *)c->gout.p, N, (double *)c->gacc64.p};
     const int ntd = p.nt / p.dtinv;
     const int mr = std::max(1, p.max_rec);
     dim3 gr_rec((mr + 127) / 128, nshots);
@@ -946,7 +952,24 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
                     auto corr = [&](auto kern) {
                         launch_dep(c->st, c->pdl, kern, dim3(gc), dim3(128), 0, c->g, Lr.S, Lr.M, sn, gr, h);
                     };
-                    if (f16s) {
+                    if (gr.acc64) {  // the sums in double (grad_acc64)
+                        if (f16s) {
+                            if (c->ac) corr(k_correlate_pairs<1, 0, 1, 1, true>);
+                            else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 1, true>);
+                            else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 1, true>);
+                            else corr(k_correlate_pairs<0, 1, 0, 1, true>);
+                        } else if (i16s) {
+                            if (c->ac) corr(k_correlate_pairs<1, 0, 1, 2, true>);
+                            else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 2, true>);
+                            else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 2, true>);
+                            else corr(k_correlate_pairs<0, 1, 0, 2, true>);
+                        } else {
+                            if (c->ac) corr(k_correlate_pairs<1, 0, 1, 0, true>);
+                            else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 0, true>);
+                            else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 0, true>);
+                            else corr(k_correlate_pairs<0, 1, 0, 0, true>);
+                        }
+                    } else if (f16s) {
                         if (c->ac) corr(k_correlate_pairs<1, 0, 1, 1>);
                         else if (c->psv && c->sh) corr(k_correlate_pairs<1, 1, 0, 1>);
                         else if (c->psv) corr(k_correlate_pairs<1, 0, 0, 1>);
@@ -970,6 +993,14 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
                                                             c->ac);
             c->launches++;
             hin_a++;
+        }
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        if (gr.acc64) {
+            const long long n = (long long)nshots * 5 * N;
+            launch_dep(c->st, c->pdl, k_acc_round, dim3((unsigned)std::min<long long>((n + 255) / 256, 4096)),
+                       dim3(256), 0, (const double *)gr.acc64, gr.acc, n);
+            c->launches++;
         }
     }
     launch_dep(c->st, c->pdl, k_assemble<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.M, gr, c->psv, c->sh, c->ac);

@@ -109,6 +109,10 @@ typedef struct ifos_params {
     int max_shots;          /* shot slots stepped together, >= 1 */
     int max_models;         /* model slots, >= 1 */
     int max_src, max_rec;   /* per-shot source / receiver capacity */
+    int grad_acc64;         /* 1: the fp32 path accumulates the correlation sums in double and
+                               rounds them to float once, before the assembly (needs fp32
+                               arithmetic, an even NX and IFOS_SNAP_F32/F16S/I16S); 0: in float,
+                               as the reference does (default) */
 } ifos_params;
 
 typedef struct ifos_ctx ifos_ctx;

@@ -268,6 +268,30 @@ def test_stage_release_wait_runs_out_cleanly():
     assert bit_equal(fresh["sections"], ref["sections"]) and bit_equal(fresh["grads"], ref["grads"])
 
 
+@pytest.mark.parametrize("fmt", ["fp32", "fp16s"])
+def test_fp64_gradient_accumulators(fmt):
+    """grad_acc64: the same per-step correlation terms summed in double and
+    rounded once.  Seismograms are untouched (bit-identical), the gradients
+    stay within the FP32 bar of the float sums, and with fp32 snapshots of
+    the fp64 run too (on a short run the summation error is far below the
+    error of the fp32 terms themselves, so either sum may land nearer the
+    fp64 one)."""
+    p, model, g, sig, adj = build_case("psv_visc_o4", nt=120)
+    runs = {}
+    for tag, kw in (("f32acc", dict(snap_format=fmt)), ("f64acc", dict(snap_format=fmt, grad_acc64=True)),
+                    ("fp64", dict(precision="fp64"))):
+        runs[tag] = gpu_shot(p, model, g, sig, adj, **kw)
+    a, b, ref = runs["f32acc"], runs["f64acc"], runs["fp64"]
+    assert bit_equal(a["sections"], b["sections"])
+    assert rel_l2(b["grads"], a["grads"]) <= TOL
+    if fmt == "fp32":  # with 2-byte snapshots the snapshot rounding dominates both
+        assert rel_l2(b["grads"][:6], ref["grads"][:6]) <= TOL
+    from ifos_b200._lib import IfosError
+    q = p.copy(nx=p.nx + 1)
+    with pytest.raises(IfosError):
+        ShotSolver(q, max_rec=g.recpos.shape[1], grad_acc64=True)  # needs an even NX
+
+
 def test_error_paths_return_status_not_fault():
     p, model, g, sig, adj = build_case("psv_el_o4")
     from ifos_b200._lib import IfosError
