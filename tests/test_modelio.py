@@ -21,7 +21,9 @@ NX, NY = 9, 7
 def _lib():
     if not os.path.exists(LIB):
         pytest.skip("oracle/_ref/libifoswriters.so is not built (make -C oracle driver)")
-    lib = C.CDLL(LIB)
+    # its own definitions first: the reference oracle library (loaded globally by other tests) defines the
+    # same globals and stubs the file merging out
+    lib = C.CDLL(LIB, mode=os.RTLD_LOCAL | os.RTLD_DEEPBIND)
     lib.matrix.restype = FPP
     lib.matrix.argtypes = [C.c_int] * 4
     lib.writemod.argtypes = [C.c_char_p, FPP, C.c_int]
