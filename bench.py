@@ -251,7 +251,11 @@ def cpu_baseline(full_nt, procs=None, ns=30):
         times = pool.map(_ref_sample, [(ns, k) for k in range(procs)])
         wall = time.perf_counter() - t0
     value = procs / wall * (ns / full_nt)
-    return {"value": value, "unit": METRIC, "cores": procs, "kind": kind, "wall_s": wall,
+    return {"value": value, "unit": METRIC, "cores": procs, "host_cores": ncpu,
+            "cores_note": ("one process per host core" if procs >= ncpu else
+                           f"{procs} of {ncpu} host cores: each process holds ~1 GB at this grid size and the "
+                           "processes are capped at 60 % of the available memory"),
+            "kind": kind, "wall_s": wall,
             "sample": f"{procs} processes x 1 shot, {ns} forward + {ns} adjoint steps each on the full 2000x600 "
                       f"grid (scaled by {ns}/{full_nt}); wall {wall:.1f} s, per-process {statistics.median(times):.1f} s",
             "library": "oracle/_ref (reference src compiled in place, gcc -O3 -std=c99)" if kind == "reference"
@@ -597,7 +601,7 @@ def main():
 
     from ifos_b200 import autotune as A
     from ifos_b200 import workloads as W
-    from ifos_b200.multigpu import shot_index
+    from ifos_b200.multigpu import reduce_rank_sums, shot_index
     from ifos_b200.solver import ShotSolver
 
     p, model, geoms = workload(args.nt)
@@ -665,8 +669,7 @@ def main():
         for k in range(args.steps):
             step_ms.append(one_step(args.warmup + k))
         if dist:
-            solver.grad_sum_device(B, grad_dev.data_ptr())
-            dist.all_reduce(grad_dev)
+            reduce_rank_sums(lambda t: solver.grad_sum_device(B, t.data_ptr()), grad_dev)
         ev1.record(stream)
         torch.cuda.synchronize(device)
     if dist:

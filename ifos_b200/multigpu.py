@@ -57,3 +57,17 @@ def sharded_sum(run_shot: Callable[[int], Tuple[Sequence, float]], nshots: int, 
     allreduce_sum(grad, group)
     allreduce_sum(mis, group)
     return grad, float(mis.item())
+
+
+def reduce_rank_sums(fill_local: Callable, out, misfit_local: float = 0.0, group=None) -> float:
+    """The reduction of a batched run over ranks: `fill_local(out)` writes
+    this rank's gradient sum into the tensor `out` on the rank's device (the
+    solver's device-side shot sum, ifos_grad_sum_device), then one all-reduce
+    of the gradients and one of the FP64 misfit.  Returns the summed
+    misfit; `out` holds the summed gradients of all ranks."""
+    import torch
+    fill_local(out)
+    allreduce_sum(out, group)
+    mis = torch.tensor([float(misfit_local)], dtype=torch.float64, device=out.device)
+    allreduce_sum(mis, group)
+    return float(mis.item())

@@ -74,3 +74,35 @@ def test_two_ranks_reproduce_single_process_sums(tmp_path):
     want_m = sum(m for _, m in per)
     assert np.linalg.norm(grad - want_g) <= 1e-6 * np.linalg.norm(want_g)
     assert abs(mis - want_m) <= 1e-12 * want_m
+
+
+def _reduce_worker(rank, world, port, out):
+    from ifos_b200.multigpu import reduce_rank_sums
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        grad = torch.zeros((5, 4, 3), dtype=torch.float32)
+        local = torch.arange(60, dtype=torch.float32).reshape(5, 4, 3) * (rank + 1)
+
+        def fill(t):  # stands in for the solver's device-side shot sum (ifos_grad_sum_device)
+            t.copy_(local)
+
+        mis = reduce_rank_sums(fill, grad, misfit_local=0.25 * (rank + 1))
+        np.save(f"{out}_{rank}.npy", grad.numpy())
+        np.save(f"{out}_{rank}_mis.npy", np.array([mis]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_bench_reduction_of_rank_sums(tmp_path):
+    """The reduction bench.py --gpus N runs after its timed steps
+    (multigpu.reduce_rank_sums: each rank's device-side gradient sum, one
+    all-reduce of the gradients and one of the misfit), with two gloo ranks:
+    every rank ends with the sum over ranks."""
+    out = str(tmp_path / "red")
+    mp.start_processes(_reduce_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
+    want = np.arange(60, dtype=np.float32).reshape(5, 4, 3) * 3
+    for r in range(2):
+        assert np.array_equal(np.load(f"{out}_{r}.npy"), want)
+        assert float(np.load(f"{out}_{r}_mis.npy")[0]) == 0.75
