@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--snap", default="fp16s", choices=["fp32", "bf16", "fp16", "fp16s", "i16s"],
                     help="snapshot format of the batched form (the plain FP32 path always stores fp32)")
     ap.add_argument("--batch", type=int, default=0, help="shots per context (0: chosen by the autotuner)")
+    ap.add_argument("--mu-grouping", default="corrected", choices=["corrected", "reference"],
+                    help="mu correlation of the batched form: the corrected grouping (ifos_params.mu_corrected) "
+                         "or the reference's expression; the plain FP32 path always uses the reference's")
     ap.add_argument("--max-batch", type=int, default=8)
     ap.add_argument("--opts", default=None,
                     help='execution options as JSON (e.g. \'{"pdl": 0, "tile_order": 1}\'); default: autotuned')
@@ -73,6 +76,8 @@ def parse():
     ap.add_argument("--serving-full", action="store_true", help="full-size serving stream (grids to 3000x1000)")
     ap.add_argument("--precision-nt", type=int, default=1200,
                     help="NT of the precision study (8000 is the precision workload's full NT)")
+    ap.add_argument("--error-only", action="store_true",
+                    help="run only the FP64 error of the workload (at --nt) and print its JSON")
     ap.add_argument("--precision-only", action="store_true",
                     help="run only the precision study (at --precision-nt) and print its JSON")
     return ap.parse_args()
@@ -281,8 +286,21 @@ def fp64_error(p, model, g, nt=None, formats=("fp32", "fp16s"), device=0):
     rng = np.random.default_rng(1)
     obs = (rng.standard_normal((1, 3, ntr, q.nt)) * 1e-9).astype(np.float32)
     out = {}
-    for tag in ("fp64",) + tuple(formats):
-        kw = dict(precision="fp64") if tag == "fp64" else ({} if tag == "fp32" else dict(snap_format=tag))
+    def solver_kw(tag):
+        """fp64 or a snapshot format, with the optional suffixes _acc64 (the
+        correlation sums in double) and _mufix (the corrected mu grouping)"""
+        base, *mods = tag.split("_")
+        kw = dict(mu_corrected="mufix" in mods)
+        if base == "fp64":
+            kw["precision"] = "fp64"
+        else:
+            kw.update(snap_format=base, grad_acc64="acc64" in mods)
+        return kw
+
+    mufix = any("mufix" in t for t in formats)
+    for tag in (("fp64",) + tuple(t for t in formats if "mufix" not in t) +
+                (("fp64_mufix",) + tuple(t for t in formats if "mufix" in t) if mufix else ())):
+        kw = solver_kw(tag)
         with ShotSolver(q, max_rec=ntr, device=device, **kw) as s:
             s.upload_model(model)
             s.setup_shot(0, g.srcpos, sig, g.recpos)
@@ -290,7 +308,7 @@ def fp64_error(p, model, g, nt=None, formats=("fp32", "fp16s"), device=0):
             l2, _ = s.residual_adjoint(obs, 1)
             gr = s.adjoint(None, 1)[0]
         out[tag] = (sec.astype(np.float64), gr.astype(np.float64), float(l2[0]))
-    ref_s, ref_g, ref_m = out["fp64"]
+    refs = {False: out["fp64"], True: out.get("fp64_mufix")}
     planes = [3, 4, 5] if q.wavetype != 2 else [8, 9]      # assembled per-shot gradients
     raw = [0, 1, 2] if q.wavetype != 2 else [6, 7]         # the correlation sums before assembly
     comps = [0, 1] if q.wavetype != 2 else [2]
@@ -298,10 +316,14 @@ def fp64_error(p, model, g, nt=None, formats=("fp32", "fp16s"), device=0):
                   f"{'vp, vs, rho' if q.wavetype != 2 else 'vs_z, rho_z'} planes (raw: the "
                   f"{'lambda, mu, rho' if q.wavetype != 2 else 'mu_z, rho_z'} correlation sums), seismograms = "
                   f"{'vx, vy' if q.wavetype != 2 else 'vz'}, misfit = FP64 L2 of the residual"}
+    names = (["vp", "vs", "rho"] if q.wavetype != 2 else ["vs_z", "rho_z"])
+    raw_names = (["lambda", "mu", "rho_raw"] if q.wavetype != 2 else ["mu_z", "rho_z_raw"])
     for tag in formats:
         s_, g_, m_ = out[tag]
+        ref_s, ref_g, ref_m = refs["mufix" in tag]  # the fp64 run with the same mu expression
         res[tag] = {"seismogram_rel_l2": _rel(s_[comps], ref_s[comps]), "gradient_rel_l2": _rel(g_[planes], ref_g[planes]),
                     "raw_gradient_rel_l2": _rel(g_[raw], ref_g[raw]),
+                    "per_plane": {nm: _rel(g_[k], ref_g[k]) for nm, k in zip(names + raw_names, planes + raw)},
                     "misfit_rel": abs(m_ - ref_m) / max(abs(ref_m), 1e-300)}
     return res
 
@@ -330,7 +352,12 @@ def precision_study(device, nt=1200):
                         ("fp16", dict(snap_format="fp16")), ("fp16s", dict(snap_format="fp16s")),
                         ("i16s", dict(snap_format="i16s")),
                         # the correlation sums in double: separates the accumulation from the propagation
-                        ("fp32_acc64", dict(grad_acc64=True)), ("i16s_acc64", dict(snap_format="i16s", grad_acc64=True))):
+                        ("fp32_acc64", dict(grad_acc64=True)), ("i16s_acc64", dict(snap_format="i16s", grad_acc64=True)),
+                        # the corrected mu grouping, against the fp64 run with the same grouping
+                        ("fp64_mufix", dict(precision="fp64", mu_corrected=True)),
+                        ("fp32_mufix", dict(mu_corrected=True)),
+                        ("fp16s_mufix", dict(snap_format="fp16s", mu_corrected=True)),
+                        ("i16s_mufix", dict(snap_format="i16s", mu_corrected=True))):
             with ShotSolver(p, max_rec=ntr, device=device, **kw) as s:
                 s.upload_model(model)
                 s.setup_shot(0, g.srcpos, sig, g.recpos)
@@ -338,10 +365,13 @@ def precision_study(device, nt=1200):
                 l2, _ = s.residual_adjoint(obs, 1)
                 gr = s.adjoint(None, 1)[0]
             runs[tag] = (sec[comps].astype(np.float64), gr[planes].astype(np.float64), float(l2[0]))
-        rs, rg, rm = runs["fp64"]
-        out[name] = {tag: {"seismogram_rel_l2": _rel(runs[tag][0], rs), "gradient_rel_l2": _rel(runs[tag][1], rg),
-                           "misfit_rel": abs(runs[tag][2] - rm) / max(abs(rm), 1e-300)}
-                     for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s", "fp32_acc64", "i16s_acc64")}
+        def row(tag):
+            rs, rg, rm = runs["fp64_mufix" if "mufix" in tag else "fp64"]
+            return {"seismogram_rel_l2": _rel(runs[tag][0], rs), "gradient_rel_l2": _rel(runs[tag][1], rg),
+                    "per_plane": {f"plane{k}": _rel(runs[tag][1][i], rg[i]) for i, k in enumerate(planes)},
+                    "misfit_rel": abs(runs[tag][2] - rm) / max(abs(rm), 1e-300)}
+        out[name] = {tag: row(tag) for tag in ("fp32", "bf16", "fp16", "fp16s", "i16s", "fp32_acc64", "i16s_acc64",
+                                               "fp32_mufix", "fp16s_mufix", "i16s_mufix")}
     return out
 
 
@@ -412,7 +442,7 @@ def plain_path(p, models, shots, device, count=2, warmup=1, roofline=False):
     return out
 
 
-def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
+def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1, mufix=True):
     """The batched form on its workload: 256 shots round-robin over the
     plain-elastic start model (400 x 160, NT 2000) and 4 seeded perturbations
     of it, stepped B at a time in one context (B and the execution options
@@ -443,7 +473,8 @@ def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
     rng = np.random.default_rng(5)
     adj = (rng.standard_normal((B, 3, ntr, p.nt)) * 1e-6).astype(np.float32)
     sigs = [W.ricker(p, g.srcpos) for _, g in shots]
-    with ShotSolver(p, max_shots=B, max_models=len(models), max_rec=ntr, snap_format=snap, device=device) as s:
+    with ShotSolver(p, max_shots=B, max_models=len(models), max_rec=ntr, snap_format=snap, mu_corrected=mufix,
+                    device=device) as s:
         s.set_options(**choice["options"])
         for i, m in enumerate(models):
             s.upload_model(m, i)
@@ -468,12 +499,12 @@ def batched_form(device, snap, max_batch=128, fdorder=4, wavetype=1):
         s.set_stream(None)
     value = len(shots) / (ms / 1e3)
     mi, g0 = shots[0]
-    err = fp64_error(p, models[mi], g0, formats=("fp32", snap), device=device)
+    err = fp64_error(p, models[mi], g0, formats=("fp32", snap, "fp32_mufix", f"{snap}_mufix"), device=device)
     physics = "plain-elastic" if wavetype == 1 else "SH elastic"
     return {"workload": f"batched {physics} 400x160 FDORDER{fdorder} NT2000 DTINV2, 256 shots over 5 models",
             "value": value, "unit": METRIC, "batch": B, "snapshots": snap, "options": choice["options"],
             "ms_all_shots": ms, "plain_fp32": plain, "speedup_vs_plain_fp32": value / plain["value"],
-            "fp64_error": err}
+            "mu_grouping": "corrected" if mufix else "reference", "fp64_error": err}
 
 
 def serving_bench(device, snap, full=False, n_requests=32, loads=(0.5, 1.0, 1.5)):
@@ -589,6 +620,12 @@ def main():
     if args.precision_only:
         print(json.dumps({"precision": precision_study(local, nt=args.precision_nt)}), flush=True)
         return 0
+    if args.error_only:
+        p, model, geoms = workload(args.nt)
+        print(json.dumps({"fp64_error": fp64_error(p, model, geoms[0], formats=(
+            "fp32", args.snap, "i16s", "fp32_acc64", "fp32_mufix", f"{args.snap}_mufix", "i16s_mufix"),
+            device=local)}), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -635,7 +672,8 @@ def main():
         sel = [B, opts]
         dist.broadcast_object_list(sel, src=0)
         B, opts = sel
-    solver = ShotSolver(p, max_shots=B, max_rec=ntr, snap_format=args.snap, device=device)
+    mufix = args.mu_grouping == "corrected"
+    solver = ShotSolver(p, max_shots=B, max_rec=ntr, snap_format=args.snap, mu_corrected=mufix, device=device)
     solver.set_options(**opts)
     solver.upload_model(model)
     stream = torch.cuda.current_stream(device)
@@ -794,15 +832,16 @@ def main():
     extra = {}
     if not args.no_error:
         try:
-            extra["fp64_error"] = fp64_error(p, model, geoms[0], formats=("fp32", args.snap), device=device)
+            extra["fp64_error"] = fp64_error(p, model, geoms[0], device=device,
+                                             formats=("fp32", args.snap, "fp32_mufix", f"{args.snap}_mufix"))
         except Exception as exc:  # report, never hide
             extra["fp64_error"] = {"error": repr(exc)}
     if world == 1:
-        for name, flag, fn in (("batched_form", args.no_batched, lambda: batched_form(device, args.snap)),
+        for name, flag, fn in (("batched_form", args.no_batched, lambda: batched_form(device, args.snap, mufix=mufix)),
                                ("batched_form_fdorder8", args.no_batched,
-                                lambda: batched_form(device, args.snap, fdorder=8)),
+                                lambda: batched_form(device, args.snap, fdorder=8, mufix=mufix)),
                                ("batched_form_fdorder12_sh", args.no_batched,
-                                lambda: batched_form(device, args.snap, fdorder=12, wavetype=2)),
+                                lambda: batched_form(device, args.snap, fdorder=12, wavetype=2, mufix=mufix)),
                                ("serving", args.no_serving,
                                 lambda: serving_bench(device, args.snap, full=args.serving_full)),
                                ("precision", args.no_error, lambda: precision_study(device, nt=args.precision_nt))):
@@ -822,6 +861,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy models, sources, residuals)",
         "config": {"workload": WORKLOAD, "grid": [p.nx, p.ny], "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
                    "dtinv": p.dtinv, "snapshots": args.snap, "shots_per_step_per_gpu": B,
+                   "mu_grouping": args.mu_grouping,
                    "execution_options": opts, "parallelism": f"shots sharded over {world} GPU(s)",
                    "l2": "inputs larger than L2 (snapshots of tens of GB + 0.2 GB state per shot); no flush"},
         "gcell_updates_per_s": 2 * cells * p.nt * total_shots / (elapsed / 1000.0) / 1e9,

@@ -44,7 +44,7 @@ class IfosParams(C.Structure):
         ("seismo", C.c_int), ("source_type", C.c_int), ("adjoint_type", C.c_int), ("dtinv", C.c_int),
         ("hi_order_corrected", C.c_int), ("precision", C.c_int), ("snap_format", C.c_int),
         ("max_shots", C.c_int), ("max_models", C.c_int), ("max_src", C.c_int), ("max_rec", C.c_int),
-        ("grad_acc64", C.c_int),
+        ("grad_acc64", C.c_int), ("mu_corrected", C.c_int),
     ]
 
 

@@ -54,6 +54,7 @@ struct KGrid {
     float inv_dh;    // 1/DH (exact when dh_pow2)
     int tile_order;  // pipelined stencils: 0 slot-major tile sequence, 1 slot-minor
     int prod_polls;  // pipelined stencils: polls of the producer's stage-release wait (0: the default limit)
+    int mu_fix;      // the mu correlation with the corrected grouping (ifos_params.mu_corrected)
 };
 
 // x / DH, exact in both branches: multiplying by the reciprocal of a power of

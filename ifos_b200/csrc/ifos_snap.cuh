@@ -163,6 +163,46 @@ struct KGrad {
     double *acc64;          // slot * 5 * n: the sums in double (grad_acc64), else NULL
 };
 
+// The correlation of an fp64 context (the error oracle): the terms of
+// src/IFOS2D.c:2379-2419 in double from double fields and snapshots, summed
+// in double (gr.acc64), so that the oracle's gradients carry no float
+// rounding at all.
+__device__ __forceinline__ void correlate_f64(const KGrid &g, const KState<double> &S, const KModel<double> &M,
+                                              const KSnap &sn, const KGrad &gr, int snap, int psv, int sh,
+                                              int acoustic, int slot, long long c, long long q) {
+    double *acc = gr.acc64 + (long long)slot * 5 * gr.n;
+    int k = 0;
+    if (psv) {
+        const double frx = snap_load<double>(sn, slot, snap, k++, q), fry = snap_load<double>(sn, slot, snap, k++, q);
+        acc[2 * gr.n + q] += (fieldp(S, slot, P_VXP1)[c] * frx) + (fieldp(S, slot, P_VYP1)[c] * fry);
+        if (!acoustic) {
+            const double fx = snap_load<double>(sn, slot, snap, k++, q), fy = snap_load<double>(sn, slot, snap, k++, q),
+                         fu = snap_load<double>(sn, slot, snap, k++, q);
+            const double sxx = fieldp(S, slot, P_SXX)[c], syy = fieldp(S, slot, P_SYY)[c],
+                         sxy = fieldp(S, slot, P_SXY)[c];
+            acc[q] += (fx + fy) * (sxx + syy);
+            const double mm = modelp(M, slot, M_MM)[c], ll = modelp(M, slot, M_LL)[c];
+            if (mm != 0.0) {
+                const double t1 = (1.0 / mm) * (fu * sxy);
+                const double t2 = (.25 * (g.mu_fix ? (fx + fy) * (sxx + syy) : fx + fy * (sxx + syy))) / ll;
+                const double t3 = (.25 * (g.mu_fix ? (fx - fy) * (sxx - syy) : fx - fy * (sxx - syy))) / mm;
+                acc[gr.n + q] += (t1 + t2) + t3;
+            }
+        } else {
+            const double fp = snap_load<double>(sn, slot, snap, k++, q);
+            acc[q] += fp * fieldp(S, slot, P_SP)[c];
+        }
+    }
+    if (sh) {
+        const double frz = snap_load<double>(sn, slot, snap, k++, q), fxz = snap_load<double>(sn, slot, snap, k++, q),
+                     fyz = snap_load<double>(sn, slot, snap, k++, q);
+        acc[4 * gr.n + q] += fieldp(S, slot, P_VZP1)[c] * frz;
+        const double *rho = modelp(M, slot, M_RHO), *u = modelp(M, slot, M_VS);
+        const double muss = rho[c] * u[c] * u[c];
+        acc[3 * gr.n + q] += (1.0 / (muss * muss)) * (fxz * fieldp(S, slot, P_SXZ)[c] + fyz * fieldp(S, slot, P_SYZ)[c]);
+    }
+}
+
 // zero-lag correlation with the stored forward wavefield (src/IFOS2D.c:2379-2419)
 template <typename T>
 __global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad gr, int snap, int psv, int sh,
@@ -174,6 +214,12 @@ __global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad g
     const int slot = blockIdx.z;
     if (i > g.nx || j > g.ny) return;
     const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1);
+    if constexpr (std::is_same<T, double>::value) {
+        if (gr.acc64) {
+            correlate_f64(g, S, M, sn, gr, snap, psv, sh, acoustic, slot, c, q);
+            return;
+        }
+    }
     float *acc = gr.acc + (long long)slot * 5 * gr.n;
     int k = 0;
     if (psv) {
@@ -187,8 +233,10 @@ __global__ void k_correlate(KGrid g, KState<T> S, KModel<T> M, KSnap sn, KGrad g
             const T mm = modelp(M, slot, M_MM)[c], ll = modelp(M, slot, M_LL)[c];
             if (mm != (T)0) {
                 const double t1 = (1.0 / (double)mm) * (double)(fu * sxy);
-                const double t2 = (.25 * (double)(fx + fy * (sxx + syy))) / (double)ll;
-                const double t3 = (.25 * (double)(fx - fy * (sxx - syy))) / (double)mm;
+                const double t2 = (.25 * (double)(g.mu_fix ? (fx + fy) * (sxx + syy) : fx + fy * (sxx + syy))) /
+                                  (double)ll;
+                const double t3 = (.25 * (double)(g.mu_fix ? (fx - fy) * (sxx - syy) : fx - fy * (sxx - syy))) /
+                                  (double)mm;
                 acc[gr.n + q] = (float)((double)acc[gr.n + q] + ((t1 + t2) + t3));
             }
         } else {
@@ -222,7 +270,7 @@ struct CorrCell {
 // grad_acc64 sums (the same terms added in double, rounded once at the end)
 template <int PSV, int SH, int AC, typename W = float>
 __device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, float ll, float rho, float u, W *w0,
-                                               W *w1, W *w2, W *w3, W *w4) {
+                                               W *w1, W *w2, W *w3, W *w4, bool mufix = false) {
     constexpr int KS = PSV ? (AC ? 3 : 5) : 0;  // first SH component
     if (PSV) {
         const float frx = a.f[0], fry = a.f[1];
@@ -232,8 +280,11 @@ __device__ __forceinline__ void correlate_cell(const CorrCell &a, float mm, floa
             *w0 += (W)(float)((fx + fy) * (a.sxx + a.syy));
             if (mm != 0.0f) {
                 const double t1 = (1.0 / (double)mm) * (double)(fu * a.sxy);
-                const double t2 = (.25 * (double)(fx + fy * (a.sxx + a.syy))) / (double)ll;
-                const double t3 = (.25 * (double)(fx - fy * (a.sxx - a.syy))) / (double)mm;
+                // mufix: the grouping the mu gradient needs (sums of forward times adjoint stresses)
+                const double t2 = (.25 * (double)(mufix ? (fx + fy) * (a.sxx + a.syy) : fx + fy * (a.sxx + a.syy))) /
+                                  (double)ll;
+                const double t3 = (.25 * (double)(mufix ? (fx - fy) * (a.sxx - a.syy) : fx - fy * (a.sxx - a.syy))) /
+                                  (double)mm;
                 *w1 = (W)((double)*w1 + ((t1 + t2) + t3));
             }
         } else {
@@ -326,10 +377,11 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
 #pragma unroll
         for (int k = 0; k < 5; k++)
             if (use[k]) w[k] = *reinterpret_cast<const double2 *>(acd + k * n);
-        correlate_cell<PSV, SH, AC, double>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x);
+        correlate_cell<PSV, SH, AC, double>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x,
+                                            g.mu_fix != 0);
         if (pair)
             correlate_cell<PSV, SH, AC, double>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y,
-                                                &w[4].y);
+                                                &w[4].y, g.mu_fix != 0);
 #pragma unroll
         for (int k = 0; k < 5; k++) {
             if (!use[k]) continue;
@@ -342,8 +394,10 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
 #pragma unroll
     for (int k = 0; k < 5; k++)
         if (use[k]) w[k] = ld2(acc + k * n);
-    correlate_cell<PSV, SH, AC>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x);
-    if (pair) correlate_cell<PSV, SH, AC>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y, &w[4].y);
+    correlate_cell<PSV, SH, AC>(a0, mm.x, ll.x, rho.x, u.x, &w[0].x, &w[1].x, &w[2].x, &w[3].x, &w[4].x, g.mu_fix != 0);
+    if (pair)
+        correlate_cell<PSV, SH, AC>(a1, mm.y, ll.y, rho.y, u.y, &w[0].y, &w[1].y, &w[2].y, &w[3].y, &w[4].y,
+                                    g.mu_fix != 0);
 #pragma unroll
     for (int k = 0; k < 5; k++) {
         if (!use[k]) continue;
@@ -352,16 +406,52 @@ __global__ void k_correlate_pairs(KGrid g, KState<float> S, KModel<float> M, KSn
     }
 }
 
-#ifndef IFOS_PIPE_FD
-// the double correlation sums rounded once to the float accumulators the
-// assembly reads (grad_acc64)
-__global__ void k_acc_round(const double *acc64, float *acc, long long n) {
-    pdl_wait();
-    pdl_launch();
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        acc[k] = (float)acc64[k];
+
+
+// The assembly of an fp64 context (the error oracle): the formulas of
+// src/IFOS2D.c:2477-2601 in double from the double sums, rounded once into
+// the float output planes.
+__device__ __forceinline__ void assemble_f64(const KGrid &g, const KModel<double> &M, const KGrad &gr, int psv,
+                                             int sh, int acoustic, int slot, long long c, long long q) {
+    const long long n = gr.n;
+    const double *acc = gr.acc64 + (long long)slot * 5 * n;
+    float *o = gr.out + (long long)slot * 10 * n;
+    const double wl = acc[q], wm = acc[n + q], wr = acc[2 * n + q], wmz = acc[3 * n + q], wrz = acc[4 * n + q];
+    o[0 * n + q] = (float)wl;
+    o[1 * n + q] = (float)wm;
+    o[2 * n + q] = (float)wr;
+    o[6 * n + q] = (float)wmz;
+    o[7 * n + q] = (float)wrz;
+    const double DT = (double)g.dt;
+    const double rho = modelp(M, slot, M_RHO)[c], u = modelp(M, slot, M_VS)[c], pi = modelp(M, slot, M_VP)[c];
+    double vp_g = 0, vs_g = 0, rho_g = 0;
+    if (psv) {
+        double lam = -DT * wl, mu = 0;
+        const double muss = !acoustic ? rho * u * u : 0;
+        const double lamss = rho * pi * pi - 2.0 * muss;
+        lam = !acoustic ? lam / (4.0 * (lamss + muss) * (lamss + muss)) : lam / ((lamss + muss) * (lamss + muss));
+        vp_g = 2.0 * pi * rho * lam;
+        if (!acoustic) {
+            mu = -DT * wm;
+            vs_g = -4.0 * rho * u * lam + 2.0 * rho * u * mu;
+        } else {
+            vs_g = wm;
+        }
+        const double rho_s = -DT * wr;
+        rho_g = !acoustic ? (pi * pi - 2.0 * u * u) * lam + u * u * mu + rho_s : (pi * pi) * lam + rho_s;
+    }
+    o[3 * n + q] = (float)vp_g;
+    o[4 * n + q] = (float)vs_g;
+    o[5 * n + q] = (float)rho_g;
+    if (sh && !acoustic) {
+        const double mu_z = -DT * wmz;
+        o[8 * n + q] = (float)(2.0 * rho * u * mu_z);
+        o[9 * n + q] = (float)(u * u * mu_z + (-DT * wrz));
+    } else {
+        o[8 * n + q] = (float)wmz;
+        o[9 * n + q] = (float)wrz;
+    }
 }
-#endif
 
 // per-shot gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2477-2601)
 template <typename T>
@@ -375,7 +465,16 @@ __global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int 
     const long long c = pidx(g, j, i), q = (long long)(j - 1) * g.nx + (i - 1), n = gr.n;
     const float *acc = gr.acc + (long long)slot * 5 * n;
     float *o = gr.out + (long long)slot * 10 * n;
-    const float wl = acc[q], wm = acc[n + q], wr = acc[2 * n + q], wmz = acc[3 * n + q], wrz = acc[4 * n + q];
+    if constexpr (std::is_same<T, double>::value) {
+        if (gr.acc64) {  // the fp64 oracle: the assembly in double from the double sums
+            assemble_f64(g, M, gr, psv, sh, acoustic, slot, c, q);
+            return;
+        }
+    }
+    const double *acd = gr.acc64 ? gr.acc64 + (long long)slot * 5 * n : nullptr;
+    // grad_acc64: the double sums rounded once, then the reference's assembly
+    auto w = [&](int k) { return acd ? (float)acd[k * n + q] : acc[k * n + q]; };
+    const float wl = w(0), wm = w(1), wr = w(2), wmz = w(3), wrz = w(4);
     o[0 * n + q] = wl;
     o[1 * n + q] = wm;
     o[2 * n + q] = wr;

@@ -353,6 +353,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     g.fdoh = p.fdorder / 2;
     g.L = p.L;
     g.quirk_hi = (p.fdorder >= 10 && !p.hi_order_corrected && (c->psv || c->ac)) ? 1 : 0;
+    g.mu_fix = p.mu_corrected ? 1 : 0;
     g.nt_total = p.nt;
     g.dt = p.dt;
     g.dh = p.dh;
@@ -454,7 +455,8 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     if ((rc = dev_alloc(c, c->sec, (size_t)S * IFOS_NS * mr * p.nt * 4))) return bail(rc);
     const long long N = (long long)p.nx * p.ny;
     if ((rc = dev_alloc(c, c->gacc, (size_t)S * 5 * N * 4))) return bail(rc);
-    if (p.grad_acc64 && (rc = dev_alloc(c, c->gacc64, (size_t)S * 5 * N * 8))) return bail(rc);
+    // the double sums: grad_acc64, and always in an fp64 context (the error oracle sums and assembles in double)
+    if ((p.grad_acc64 || p.precision == 1) && (rc = dev_alloc(c, c->gacc64, (size_t)S * 5 * N * 8))) return bail(rc);
     if ((rc = dev_alloc(c, c->gout, (size_t)S * IFOS_NG * N * 4))) return bail(rc);
     if ((rc = dev_alloc(c, c->bad, sizeof(int)))) return bail(rc);
     if ((rc = dev_alloc(c, c->dot_partial, 1024 * sizeof(double)))) return bail(rc);
@@ -993,14 +995,6 @@ static int adjoint_t(ifos_ctx *c, int nshots) {
                                                             c->ac);
             c->launches++;
             hin_a++;
-        }
-    }
-    if constexpr (std::is_same<T, float>::value) {
-        if (gr.acc64) {
-            const long long n = (long long)nshots * 5 * N;
-            launch_dep(c->st, c->pdl, k_acc_round, dim3((unsigned)std::min<long long>((n + 255) / 256, 4096)),
-                       dim3(256), 0, (const double *)gr.acc64, gr.acc, n);
-            c->launches++;
         }
     }
     launch_dep(c->st, c->pdl, k_assemble<T>, dim3(Lr.grd), dim3(Lr.blk), 0, c->g, Lr.M, gr, c->psv, c->sh, c->ac);

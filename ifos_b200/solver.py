@@ -28,7 +28,7 @@ def _f32(a):
 
 
 def make_params(p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=1, precision="fp32",
-                snap_format="fp32", hi_order_corrected=False, grad_acc64=False) -> IfosParams:
+                snap_format="fp32", hi_order_corrected=False, grad_acc64=False, mu_corrected=False) -> IfosParams:
     c = IfosParams()
     _lib.load().ifos_params_default(C.byref(c))
     for name in ("nx", "ny", "nt", "dh", "dt", "fdorder", "maxrelerror", "fw", "free_surf", "boundary", "vppml",
@@ -43,6 +43,7 @@ def make_params(p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=
     c.max_shots, c.max_models = int(max_shots), int(max_models)
     c.max_src, c.max_rec = int(max_src), int(max_rec)
     c.grad_acc64 = 1 if grad_acc64 else 0
+    c.mu_corrected = 1 if mu_corrected else 0
     return c
 
 
@@ -107,12 +108,14 @@ class ShotSolver:
     """One device context: ``max_shots`` shot slots stepped together."""
 
     def __init__(self, p: ShotParams, *, max_shots=1, max_models=1, max_src=1, max_rec=1, snapshots=True,
-                 precision="fp32", snap_format="fp32", hi_order_corrected=False, grad_acc64=False, device=0):
+                 precision="fp32", snap_format="fp32", hi_order_corrected=False, grad_acc64=False,
+                 mu_corrected=False, device=0):
         self.p = p
         self.lib = _lib.load()
         self.params = make_params(p, max_shots=max_shots, max_models=max_models, max_src=max_src, max_rec=max_rec,
                                   precision=precision, snap_format=snap_format,
-                                  hi_order_corrected=hi_order_corrected, grad_acc64=grad_acc64)
+                                  hi_order_corrected=hi_order_corrected, grad_acc64=grad_acc64,
+                                  mu_corrected=mu_corrected)
         self.max_shots, self.max_rec, self.max_src = int(max_shots), int(max_rec), int(max_src)
         self._ctx = C.c_void_p()
         self._inflight = []  # host arrays of asynchronous fetches not yet waited for

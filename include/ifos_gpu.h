@@ -113,6 +113,10 @@ typedef struct ifos_params {
                                rounds them to float once, before the assembly (needs fp32
                                arithmetic, an even NX and IFOS_SNAP_F32/F16S/I16S); 0: in float,
                                as the reference does (default) */
+    int mu_corrected;       /* 1: the mu correlation as (f_xx+f_yy)(s_xx+s_yy) and (f_xx-f_yy)(s_xx-s_yy)
+                               (a documented deviation: src/IFOS2D.c:2398-2404 multiplies before it
+                               adds, so the forward stresses enter alone and cancel only over time);
+                               0: the reference's expression (default) */
 } ifos_params;
 
 typedef struct ifos_ctx ifos_ctx;

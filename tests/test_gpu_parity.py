@@ -292,6 +292,26 @@ def test_fp64_gradient_accumulators(fmt):
         ShotSolver(q, max_rec=g.recpos.shape[1], grad_acc64=True)  # needs an even NX
 
 
+def test_corrected_mu_grouping():
+    """mu_corrected (a documented deviation): the mu correlation as
+    (f_xx+f_yy)(s_xx+s_yy) and (f_xx-f_yy)(s_xx-s_yy).  Only the mu sum and
+    what is assembled from it (vs, rho) change; the lambda and rho sums, vp
+    and the seismograms are bit-identical to the reference grouping; and
+    with it the fp32 mu gradient is close to the fp64 run of the same
+    grouping (the reference grouping's forward-only terms, which cancel only
+    over time, are gone)."""
+    p, model, g, sig, adj = build_case("psv_visc_o4", nt=120)
+    ref = gpu_shot(p, model, g, sig, adj)
+    fix = gpu_shot(p, model, g, sig, adj, mu_corrected=True)
+    f64 = gpu_shot(p, model, g, sig, adj, mu_corrected=True, precision="fp64")
+    assert bit_equal(ref["sections"], fix["sections"])
+    for k in (0, 2, 3):  # lambda and rho sums, vp
+        assert bit_equal(ref["grads"][k], fix["grads"][k]), k
+    assert not np.array_equal(ref["grads"][1], fix["grads"][1])
+    for k in (1, 4, 5):
+        assert rel_l2(fix["grads"][k], f64["grads"][k]) <= TOL, k
+
+
 def test_error_paths_return_status_not_fault():
     p, model, g, sig, adj = build_case("psv_el_o4")
     from ifos_b200._lib import IfosError
