@@ -55,6 +55,7 @@ struct KGrid {
     int tile_order;  // pipelined stencils: 0 slot-major tile sequence, 1 slot-minor
     int prod_polls;  // pipelined stencils: polls of the producer's stage-release wait (0: the default limit)
     int mu_fix;      // the mu correlation with the corrected grouping (ifos_params.mu_corrected)
+    int lame;        // PARAMETERIZATION 3: the model planes hold lambda and mu, the assembly stops at the moduli
 };
 
 // x / DH, exact in both branches: multiplying by the reciprocal of a power of

@@ -208,36 +208,41 @@ bool build_model(const ifos_params &p, const float *vp, const float *vs, const f
         if (!o.tau_uniform) o.taup = tp;
         return true;
     }
+    // PARAMETERIZATION 3: PI and U hold lambda and mu themselves; the
+    // reference's correlation weights (mm, ll) keep their vp/vs form under
+    // both parameterizations (src/IFOS2D.c:2395-2396 has no branch)
+    const bool lame = p.parameterization == 3;
     o.uipjp.resize(N);
     o.f_el.resize(N);
     o.g_el.resize(N);
     o.mm.resize(N);
     o.ll.resize(N);
     for (int j = 1; j <= NY; j++)
-        for (int i = 1; i <= NX; i++) {  // src/av_mue.c:45-61
+        for (int i = 1; i <= NX; i++) {  // src/av_mue.c:28-61
             size_t k = gi(j, i), k2 = gi(j, i + 1), k3 = gi(j + 1, i), k4 = gi(j + 1, i + 1);
-            float u1 = R[k] * U[k] * U[k];
-            float u2 = R[k2] * U[k2] * U[k2];
-            float u3 = R[k3] * U[k3] * U[k3];
-            float u4 = R[k4] * U[k4] * U[k4];
+            float u1 = lame ? U[k] : R[k] * U[k] * U[k];
+            float u2 = lame ? U[k2] : R[k2] * U[k2] * U[k2];
+            float u3 = lame ? U[k3] : R[k3] * U[k3] * U[k3];
+            float u4 = lame ? U[k4] : R[k4] * U[k4] * U[k4];
             float v = 4.0 / ((1.0 / u1) + (1.0 / u2) + (1.0 / u3) + (1.0 / u4));
             if ((u1 == 0.0) || (u2 == 0.0) || (u3 == 0.0) || (u4 == 0.0)) v = 0.0;
             o.uipjp[k] = v;
         }
     for (size_t k = 0; k < N; k++) {
-        o.f_el[k] = R[k] * U[k] * U[k];                          // src/update_s_elastic_PML.c:229
-        o.g_el[k] = R[k] * ((PI[k] * PI[k]) - 2 * U[k] * U[k]);  // :230
-        float muss = R[k] * U[k] * U[k];                         // src/IFOS2D.c:2395-2396
+        // src/update_s_elastic_PML.c:224-230 (and the SH update's f)
+        o.f_el[k] = lame ? U[k] : R[k] * U[k] * U[k];
+        o.g_el[k] = lame ? PI[k] : R[k] * ((PI[k] * PI[k]) - 2 * U[k] * U[k]);
+        float muss = R[k] * U[k] * U[k];  // src/IFOS2D.c:2395-2396
         float lamss = R[k] * PI[k] * PI[k] - 2.0 * muss;
         o.mm[k] = (U[k] > 0.0) ? muss * muss : 0.0f;
         o.ll[k] = (lamss + muss) * (lamss + muss);
     }
-    // free-surface row coefficients, elastic (src/surface_elastic_PML.c:94-99)
+    // free-surface row coefficients, elastic (src/surface_elastic_PML.c:94-100)
     o.srf_fjm.resize(NX);
     o.srf_g.resize(NX);
     for (int i = 0; i < NX; i++) {
-        o.srf_fjm[i] = R[i] * U[i] * U[i] * 2.0;
-        o.srf_g[i] = R[i] * ((PI[i] * PI[i]) - 2 * U[i] * U[i]);
+        o.srf_fjm[i] = lame ? U[i] * 2.0 : R[i] * U[i] * U[i] * 2.0;
+        o.srf_g[i] = lame ? PI[i] : R[i] * ((PI[i] * PI[i]) - 2 * U[i] * U[i]);
     }
     if (!p.L) return true;
 
@@ -258,9 +263,10 @@ bool build_model(const ifos_params &p, const float *vp, const float *vs, const f
     o.muipjp_r.resize(N);
     const float DT = p.dt;
     const int L = p.L;
-    for (size_t k = 0; k < N; k++) {  // src/prepare_update_s.c:50-60
-        float mu = (U[k] * U[k] * R[k]) / (1.0 + vs_.sumu * ts[k]);
-        float pi = (PI[k] * PI[k] * R[k]) / (1.0 + vs_.sumpi * tp[k]);
+    for (size_t k = 0; k < N; k++) {  // src/prepare_update_s.c:60-93
+        float mu = lame ? U[k] / (1.0 + vs_.sumu * ts[k]) : (U[k] * U[k] * R[k]) / (1.0 + vs_.sumu * ts[k]);
+        float pi = lame ? (PI[k] + 2 * U[k]) / (1.0 + vs_.sumpi * tp[k])
+                        : (PI[k] * PI[k] * R[k]) / (1.0 + vs_.sumpi * tp[k]);
         float muipjp = o.uipjp[k] / (1.0 + vs_.sumu * tsij[k]);
         o.fipjp_v[k] = muipjp * DT * (1.0 + L * tsij[k]);
         o.f_v[k] = mu * DT * (1.0 + L * ts[k]);
@@ -280,12 +286,13 @@ bool build_model(const ifos_params &p, const float *vp, const float *vs, const f
         o.taup = tp;
         o.tausipjp = tsij;
     }
-    // visco free-surface row (src/surface_PML.c:127-147)
+    // visco free-surface row (src/surface_PML.c:125-147)
     o.srf_djm.resize(NX);
     o.srf_e.resize(NX);
     for (int i = 0; i < NX; i++) {
-        float mu = (U[i] * U[i] * R[i]) / (1.0 + vs_.sumu * ts[i]);
-        float pi = (PI[i] * PI[i] * R[i]) / (1.0 + vs_.sumpi * tp[i]);
+        float mu = lame ? U[i] / (1.0 + vs_.sumu * ts[i]) : (U[i] * U[i] * R[i]) / (1.0 + vs_.sumu * ts[i]);
+        float pi = lame ? (PI[i] + 2 * U[i]) / (1.0 + vs_.sumpi * tp[i])
+                        : (PI[i] * PI[i] * R[i]) / (1.0 + vs_.sumpi * tp[i]);
         o.srf_fjm[i] = mu * 2.0 * (1.0 + L * ts[i]);
         o.srf_g[i] = pi * (1.0 + L * tp[i]);
         o.srf_djm[i] = 2.0 * mu * ts[i];

@@ -423,6 +423,14 @@ __device__ __forceinline__ void assemble_f64(const KGrid &g, const KModel<double
     o[6 * n + q] = (float)wmz;
     o[7 * n + q] = (float)wrz;
     const double DT = (double)g.dt;
+    if (g.lame) {  // PARAMETERIZATION 3: the lambda, mu and rho gradients (src/IFOS2D.c:2498-2608)
+        o[3 * n + q] = psv ? (float)(-DT * wl) : 0.0f;
+        o[4 * n + q] = psv ? (float)(-DT * wm) : 0.0f;
+        o[5 * n + q] = psv ? (float)(-DT * wr) : 0.0f;
+        o[8 * n + q] = sh ? (float)(-DT * wmz) : (float)wmz;
+        o[9 * n + q] = sh ? (float)(-DT * wrz) : (float)wrz;
+        return;
+    }
     const double rho = modelp(M, slot, M_RHO)[c], u = modelp(M, slot, M_VS)[c], pi = modelp(M, slot, M_VP)[c];
     double vp_g = 0, vs_g = 0, rho_g = 0;
     if (psv) {
@@ -453,7 +461,7 @@ __device__ __forceinline__ void assemble_f64(const KGrid &g, const KModel<double
     }
 }
 
-// per-shot gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2477-2601)
+// per-shot gradient assembly, PARAMETERIZATION 1 and 3 (src/IFOS2D.c:2477-2608)
 template <typename T>
 __global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int acoustic) {
     pdl_wait();
@@ -481,6 +489,18 @@ __global__ void k_assemble(KGrid g, KModel<T> M, KGrad gr, int psv, int sh, int 
     o[6 * n + q] = wmz;
     o[7 * n + q] = wrz;
     const float DT = g.dt;
+    if (g.lame) {
+        // PARAMETERIZATION 3 (src/IFOS2D.c:2498-2500, :2527-2530, :2551-2554,
+        // :2581-2584, :2605-2608): each gradient is -DT times its sum; the
+        // reference leaves the vp / vs / rho planes as zero where the wave type
+        // is not modelled, and the SH planes as the raw sums
+        o[3 * n + q] = psv ? -DT * wl : 0.0f;
+        o[4 * n + q] = psv ? -DT * wm : 0.0f;
+        o[5 * n + q] = psv ? -DT * wr : 0.0f;
+        o[8 * n + q] = sh ? -DT * wmz : wmz;
+        o[9 * n + q] = sh ? -DT * wrz : wrz;
+        return;
+    }
     const float rho = (float)modelp(M, slot, M_RHO)[c], u = (float)modelp(M, slot, M_VS)[c],
                 pi = (float)modelp(M, slot, M_VP)[c];
     float vp_g = 0, vs_g = 0, rho_g = 0;

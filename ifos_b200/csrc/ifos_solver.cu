@@ -116,7 +116,15 @@ static int check_params(const ifos_params &p, std::string &why) {
     if (p.L < 0 || p.L > IFOS_MAX_L) return bad("L must be 0..8");
     if (p.wavetype < 1 || p.wavetype > 3) return bad("WAVETYPE must be 1, 2 or 3");
     if (p.acoustic && p.wavetype != 1) return bad("acoustic modelling is P-SV only");
-    if (p.parameterization != 1) return bad("only PARAMETERIZATION=1 is implemented");
+    // PARAMETERIZATION 2 has no branch in the reference's stress updates, av_mue or
+    // prepare_update_s (src/update_s_elastic_PML.c:132-137 leave f and g unset), and
+    // acoustic PARAMETERIZATION 3 none in update_p_PML (src/update_p_PML.c:96-98):
+    // no run of the reference defines those results
+    if (p.parameterization == 2)
+        return bad("PARAMETERIZATION=2 is not defined by the reference's stress updates; use 1 or 3");
+    if (p.parameterization != 1 && p.parameterization != 3) return bad("PARAMETERIZATION must be 1 or 3");
+    if (p.parameterization == 3 && p.acoustic)
+        return bad("acoustic modelling has no PARAMETERIZATION=3 branch in the reference; use 1");
     if (p.velocity != 0) return bad("only VELOCITY=0 is implemented");
     if (p.dtinv < 1 || p.nt % p.dtinv) return bad("NT must be a multiple of DTINV");
     if (p.seismo < 0 || p.seismo > 5) return bad("SEISMO must be 0..5");
@@ -354,6 +362,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     g.L = p.L;
     g.quirk_hi = (p.fdorder >= 10 && !p.hi_order_corrected && (c->psv || c->ac)) ? 1 : 0;
     g.mu_fix = p.mu_corrected ? 1 : 0;
+    g.lame = p.parameterization == 3 ? 1 : 0;
     g.nt_total = p.nt;
     g.dt = p.dt;
     g.dh = p.dh;

@@ -126,8 +126,13 @@ class ShotParams:
             raise ValueError("WAVETYPE must be 1, 2 or 3")
         if self.acoustic and self.wavetype != 1:
             raise ValueError("acoustic modelling is P-SV only (WAVETYPE=1)")
-        if self.parameterization != 1:
-            raise ValueError("the device path implements PARAMETERIZATION=1 (vp, vs, rho)")
+        if self.parameterization == 2:
+            # src/update_s_elastic_PML.c:132-137 and src/av_mue.c set nothing for 2
+            raise ValueError("PARAMETERIZATION=2 is not defined by the reference's stress updates; use 1 or 3")
+        if self.parameterization not in (1, 3):
+            raise ValueError("PARAMETERIZATION must be 1 (vp, vs, rho) or 3 (lambda, mu, rho)")
+        if self.parameterization == 3 and self.acoustic:
+            raise ValueError("acoustic modelling has no PARAMETERIZATION=3 branch in the reference (src/update_p_PML.c)")
         if self.velocity != 0:
             raise ValueError("the device path implements VELOCITY=0")
         if self.seismo not in (0, 1, 2, 3, 4, 5):

@@ -338,7 +338,8 @@ class ShotSolver:
     def mat_change_test(self, model, direction, eps_scale, iter, itest=1, start=None, lbfgs=False, **limits):
         """Test model of a step-length trial (itest != 0), or the model update
         itself (itest 0), as src/calc_mat_change_test.c computes it on one
-        rank (PARAMETERIZATION 1).  model, direction and start are dicts of
+        rank (PARAMETERIZATION 1 or 3: one update serves both, :228).  model,
+        direction and start are dicts of
         NY x NX planes: vp, vs, rho; the search directions are the driver's
         waveconv (vp), waveconv_u (vs) and waveconv_rho (rho).  `limits`
         holds the remaining fields of ifos_mat_change (inv_vp_iter,

@@ -411,16 +411,23 @@ def ricker(p: ShotParams, srcpos: np.ndarray) -> np.ndarray:
 
 
 def write_model(model: dict, prefix: str) -> None:
-    """Write vp/vs/rho (and qp/qs when the model has them) as the reference
-    reads them: raw float32, x outer, y inner (src/readmod_elastic.c,
-    src/readmod.c loop order)."""
-    for key in ("vp", "vs", "rho", "qp", "qs"):
+    """Write vp/vs/rho (lam/mu for PARAMETERIZATION 3; qp/qs when the model
+    has them) as the reference reads them: raw float32, x outer, y inner
+    (src/readmod_elastic.c, src/readmod.c loop order)."""
+    for key in ("vp", "vs", "lam", "mu", "rho", "qp", "qs"):
         if key in model:
             np.ascontiguousarray(model[key].T, dtype=np.float32).tofile(f"{prefix}.{key}")
 
 
-def read_model(prefix: str, nx: int, ny: int, tau: float = None, wavetype: int = 1) -> dict:
-    """vp, vs, rho as NY x NX planes.  With `tau` (TAU, the viscoelastic
+def read_model(prefix: str, nx: int, ny: int, tau: float = None, wavetype: int = 1,
+               parameterization: int = 1) -> dict:
+    """vp, vs, rho as NY x NX planes.  Under PARAMETERIZATION 3 the readers
+    take lambda and mu from the .lam and .mu files instead
+    (src/readmod_elastic.c:69-88, src/readmod.c:103-138) into the same pi and
+    u slots, so the planes come back under the keys "vp" and "vs" -- the
+    arguments of ifos_model_upload, which hold lambda and mu under 3; the
+    .lam file must exist even for an SH model, whose reader opens it without
+    reading it.  With `tau` (TAU, the viscoelastic
     reader of src/readmod.c:140-205) also taup and taus: 2/Q from the .qp /
     .qs files where they exist (the division in double, stored as float),
     else TAU.  As src/readmod.c:59-77 and :146-160 do, the .vp / .qp files
@@ -439,7 +446,13 @@ def read_model(prefix: str, nx: int, ny: int, tau: float = None, wavetype: int =
         return np.ascontiguousarray(a.reshape(nx, ny).T)
 
     psv = wavetype in (1, 3)
-    out = {key: plane(key) for key in (("vp", "vs", "rho") if psv else ("vs", "rho"))}
+    if parameterization == 3:
+        if not os.path.exists(f"{prefix}.lam"):
+            raise FileNotFoundError(f"could not open model file for Lame parameter lambda: {prefix}.lam")
+        files = {"vp": "lam", "vs": "mu", "rho": "rho"}
+    else:
+        files = {"vp": "vp", "vs": "vs", "rho": "rho"}
+    out = {key: plane(files[key]) for key in (("vp", "vs", "rho") if psv else ("vs", "rho"))}
     if tau is not None:
         for q, t in ((("qp", "taup"),) if psv else ()) + (("qs", "taus"),):
             if os.path.exists(f"{prefix}.{q}"):

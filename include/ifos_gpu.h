@@ -6,7 +6,7 @@
  *                       psource, surface_*_PML, seismo_ssg, snapshot store)
  *   adjoint time loop   src/IFOS2D.c:2224-2438  (same kernels with sw=1 and the
  *                       zero-lag correlation at :2379-2419)
- *   gradient assembly   src/IFOS2D.c:2471-2611  (PARAMETERIZATION=1)
+ *   gradient assembly   src/IFOS2D.c:2471-2611  (PARAMETERIZATION 1 and 3)
  *   model set-up        src/IFOS2D.c:906-943 (matcopy_elastic, av_mue, av_rho,
  *                       av_tau, prepare_update_s) and :816 (PML_pro)
  * The reference exposes these as void C functions over float** arrays plus
@@ -95,7 +95,12 @@ typedef struct ifos_params {
     float fl[IFOS_MAX_L];
     int wavetype;         /* 1 P-SV, 2 SH, 3 both */
     int acoustic;         /* 1: pressure formulation (WAVETYPE 1 only) */
-    int parameterization; /* must be 1 (vp, vs, rho) */
+    int parameterization; /* 1: vp, vs, rho; 3: lambda, mu, rho (elastic and visco,
+                             not acoustic): the vp and vs planes of ifos_model_upload
+                             then hold lambda and mu, as the reference's ppi and pu
+                             do, and the vp / vs / rho gradients are the lambda / mu /
+                             rho ones (src/IFOS2D.c:2498-2608).  2 is rejected: the
+                             reference's stress updates leave it undefined */
     int velocity;         /* must be 0 */
     int seismo;           /* 0..5 as SEISMO */
     int source_type;      /* default forward source type */
@@ -140,7 +145,8 @@ int ifos_status(ifos_ctx *ctx);
 /* Bytes of device memory a context with these parameters needs. */
 size_t ifos_ctx_bytes(const ifos_params *p, int with_snapshots);
 
-/* Upload model `model` (vp, vs, rho; taup/taus may be NULL meaning TAU) and
+/* Upload model `model` (vp, vs, rho, or lambda, mu, rho under PARAMETERIZATION
+ * 3; taup/taus may be NULL meaning TAU) and
  * rebuild its coefficients: ghost ring, rip/rjp, uipjp, viscoelastic
  * coefficients.  Replaces src/IFOS2D.c:906-943 / :3240-3265. */
 int ifos_model_upload(ifos_ctx *ctx, int model, const float *vp, const float *vs, const float *rho,
@@ -331,7 +337,8 @@ int ifos_taper_grad_shot(ifos_ctx *ctx, int nshots, const float *src_xy, float s
 int ifos_median_smooth(ifos_ctx *ctx, float *mat, int filt_size);
 
 /* Test model of a step-length trial, or the model update itself
- * (src/calc_mat_change_test.c:26-334, PARAMETERIZATION 1, one rank): each
+ * (src/calc_mat_change_test.c:26-334, PARAMETERIZATION 1 or 3, which share
+ * the update at :228, one rank): each
  * parameter's step is eps_scale * max(model) / max|search direction| (0
  * before its INV_*_ITER iteration; eps_scale itself under unnormalised
  * L-BFGS steps), then the reference's bounds, Vp/Vs ratio, limited-update

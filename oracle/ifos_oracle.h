@@ -36,7 +36,7 @@ typedef struct orc_cfg {
     float fl[ORC_MAX_L];
     int wavetype;          /* 1 P-SV, 2 SH, 3 both */
     int acoustic;
-    int parameterization;  /* 1: vp, vs, rho */
+    int parameterization;  /* 1: vp, vs, rho; 3: lambda, mu, rho (compiled reference only) */
     int velocity;          /* 0: displacement-type snapshots (stress) */
     int seismo;            /* 1..5 */
     int source_type;       /* forward source mechanism: 1 explosive, 2/3 force x/y, 4 rotated */

@@ -13,7 +13,9 @@
  *           seismo_ssg, snapshot store               (src/IFOS2D.c:1651-1894)
  *   adjoint the same kernels with sw=1 + zero-lag correlation
  *                                                    (src/IFOS2D.c:2224-2438)
- *   gradient assembly, PARAMETERIZATION=1            (src/IFOS2D.c:2471-2611)
+ *   gradient assembly, PARAMETERIZATION 1 and 3      (src/IFOS2D.c:2471-2611)
+ * The propagation kernels read PARAMETERIZATION from the globals themselves;
+ * the assembly below follows the driver's branches for 1 and 3.
  */
 #include "fd.h"
 #include "globvar.h"
@@ -512,7 +514,8 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
         if (io->adj_fields)
             for (int k = 0; k < ORC_NF; k++) put_plane(PLANE(io->adj_fields, k, NX, NY), fl[k], NX, NY);
 
-        /* gradient assembly, PARAMETERIZATION=1 (src/IFOS2D.c:2471-2611) */
+        /* gradient assembly (src/IFOS2D.c:2471-2611); PARAMETERIZATION 3 keeps
+           each -DT-scaled sum (:2498-2500, :2527-2530, :2551-2554, :2581-2584, :2605-2608) */
         if (io->grads) {
             float **lam = MAT(), **mu = MAT(), **rho_s = MAT(), **mu_z = MAT(), **rho_s_z = MAT();
             put_plane(PLANE(io->grads, ORC_G_LAM_RAW, NX, NY), wc_shot, NX, NY);
@@ -524,6 +527,10 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
                 for (int j = 1; j <= NY; j++)
                     for (int i = 1; i <= NX; i++) {
                         lam[j][i] = -DT * wc_shot[j][i];
+                        if (PARAMETERIZATION == 3) {
+                            wc_shot[j][i] = lam[j][i];
+                            continue;
+                        }
                         float muss = !ACOUSTIC ? prho[j][i] * pu[j][i] * pu[j][i] : 0;
                         float lamss = prho[j][i] * ppi[j][i] * ppi[j][i] - 2.0 * muss;
                         if (!ACOUSTIC)
@@ -536,13 +543,18 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
                     for (int j = 1; j <= NY; j++)
                         for (int i = 1; i <= NX; i++) {
                             mu[j][i] = -DT * wc_u_shot[j][i];
-                            wc_u_shot[j][i] = -4.0 * prho[j][i] * pu[j][i] * lam[j][i] +
-                                              2.0 * prho[j][i] * pu[j][i] * mu[j][i];
+                            if (PARAMETERIZATION == 3)
+                                wc_u_shot[j][i] = mu[j][i];
+                            else
+                                wc_u_shot[j][i] = -4.0 * prho[j][i] * pu[j][i] * lam[j][i] +
+                                                  2.0 * prho[j][i] * pu[j][i] * mu[j][i];
                         }
                 for (int j = 1; j <= NY; j++)
                     for (int i = 1; i <= NX; i++) {
                         rho_s[j][i] = -DT * wc_rho_shot[j][i];
-                        if (!ACOUSTIC)
+                        if (PARAMETERIZATION == 3)
+                            wc_rho_shot[j][i] = rho_s[j][i];
+                        else if (!ACOUSTIC)
                             wc_rho_shot[j][i] = ((ppi[j][i] * ppi[j][i]) - (2.0 * pu[j][i] * pu[j][i])) * lam[j][i] +
                                                 pu[j][i] * pu[j][i] * mu[j][i] + rho_s[j][i];
                         else
@@ -553,12 +565,13 @@ int orc_run_shot(const orc_cfg *c, orc_shot_io *io) {
                 for (int j = 1; j <= NY; j++)
                     for (int i = 1; i <= NX; i++) {
                         mu_z[j][i] = -DT * wc_u_z[j][i];
-                        wc_u_z[j][i] = (2.0 * prho[j][i] * pu[j][i] * mu_z[j][i]);
+                        wc_u_z[j][i] = PARAMETERIZATION == 3 ? mu_z[j][i] : (2.0 * prho[j][i] * pu[j][i] * mu_z[j][i]);
                     }
                 for (int j = 1; j <= NY; j++)
                     for (int i = 1; i <= NX; i++) {
                         rho_s_z[j][i] = -DT * wc_rho_z[j][i];
-                        wc_rho_z[j][i] = ((pu[j][i] * pu[j][i] * mu_z[j][i]) + rho_s_z[j][i]);
+                        wc_rho_z[j][i] = PARAMETERIZATION == 3 ? rho_s_z[j][i]
+                                                               : ((pu[j][i] * pu[j][i] * mu_z[j][i]) + rho_s_z[j][i]);
                     }
             }
             put_plane(PLANE(io->grads, ORC_G_VP, NX, NY), wc_shot, NX, NY);

@@ -946,6 +946,7 @@ int orc_run_shot(const orc_cfg *cfg, orc_shot_io *io) {
     g->fdoh = cfg->fdorder / 2;
     g->psv = cfg->wavetype == 1 || cfg->wavetype == 3;
     g->sh = cfg->wavetype == 2 || cfg->wavetype == 3;
+    if (cfg->parameterization != 1) return 3; /* the restatement covers vp, vs, rho only */
     if (orc_fd_coeffs(cfg, g->hc)) return 1;
     if (g->fdoh + 1 > H) return 2;
     float *prof[20];

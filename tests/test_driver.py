@@ -3,7 +3,8 @@ three ways on the same inputs (tests/driver_case.py):
 
 * stock: the reference's own sources compiled whole (oracle/_ref/IFOS2D);
 * compat: the same driver linked against libifos_compat.so in place of its
-  per-kernel sources (oracle/_ref/IFOS2D_compat; INTEGRATION.md, part A);
+  per-kernel sources (oracle/_ref/IFOS2D_compat, linked as the Makefile's
+  `driver` target shows);
 * shot ABI: the forward and adjoint of every shot through libifos_b200.so,
   from the same parameter, model, source, receiver and observed-data files.
 

@@ -152,12 +152,15 @@ def test_seismogram_files_match_saveseis_glob(kind, seismo, wavetype, adjoint_ty
         assert np.array_equal(a[:, :210], b[:, :210]) and np.array_equal(a[:, 240:], b[:, 240:]), path
 
 
-@pytest.mark.parametrize("with_qs,wavetype", [(True, 1), (False, 1), (True, 2)])
-def test_viscoelastic_model_reader_matches_readmod(with_qs, wavetype):
+@pytest.mark.parametrize("with_qs,wavetype,param", [(True, 1, 1), (False, 1, 1), (True, 2, 1), (True, 1, 3),
+                                                   (False, 2, 3)])
+def test_viscoelastic_model_reader_matches_readmod(with_qs, wavetype, param):
     """vp, vs, rho and the relaxation planes of a viscoelastic model as
     src/readmod.c reads them: taup = 2/qp, taus = 2/qs from the .qp / .qs
     files, TAU where a Q file is missing (the .qs file left out here).  An SH
-    model (WAVETYPE 2) has no .vp / .qp file and no taup plane."""
+    model (WAVETYPE 2) has no .vp / .qp file and no taup plane.  Under
+    PARAMETERIZATION 3 the .lam and .mu files take the places of .vp and .vs
+    (the .lam file present but unread for SH)."""
     from ifos_b200 import workloads as W
     ref, _ = H.libs()
     rng = np.random.default_rng(21)
@@ -168,11 +171,17 @@ def test_viscoelastic_model_reader_matches_readmod(with_qs, wavetype):
          "qp": rng.uniform(10, 200, (ny, nx)).astype(np.float32)}
     if with_qs:
         m["qs"] = rng.uniform(10, 100, (ny, nx)).astype(np.float32)
+    if param == 3:
+        m["lam"] = (m["rho"] * (m["vp"] ** 2 - 2 * m["vs"] ** 2)).astype(np.float32)
+        m["mu"] = (m["rho"] * m["vs"] ** 2).astype(np.float32)
+        del m["vp"], m["vs"]
+        if wavetype == 2:
+            m["lam"] = np.zeros(3, np.float32)  # opened, never read
     if wavetype == 2:
-        del m["vp"], m["qp"]
+        m.pop("vp", None), m.pop("qp")
     prefix = os.path.join(tempfile.mkdtemp(prefix="md"), "m")
     W.write_model(m, prefix)
-    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=wavetype, PARAMETERIZATION=1, L=2, MYID=1, DT=1e-3,
+    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=wavetype, PARAMETERIZATION=param, L=2, MYID=1, DT=1e-3,
                   FL=[5.0, 30.0])
     # IDX / IDY step the write-back loops of src/matrix_operations.c:33-34 (0 would never end)
     for name, v in (("NXG", nx), ("NYG", ny), ("IDX", 1), ("IDY", 1)):
@@ -191,11 +200,50 @@ def test_viscoelastic_model_reader_matches_readmod(with_qs, wavetype):
     libc.fclose(log)
     want = {k: np.array([[mats[q][j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
             for q, k in enumerate(("rho", "vp", "vs", "taus", "taup")) if wavetype != 2 or k not in ("vp", "taup")}
-    got = W.read_model(prefix, nx, ny, tau=tau, wavetype=wavetype)
+    got = W.read_model(prefix, nx, ny, tau=tau, wavetype=wavetype, parameterization=param)
     assert sorted(got) == sorted(want)
     for k, v in want.items():
         assert np.array_equal(got[k].view(np.int32), v.view(np.int32)), k
     assert with_qs or (got["taus"] == np.float32(tau)).all()
+    if param == 3:
+        assert np.array_equal(got["vs"], m["mu"])
+
+
+@pytest.mark.parametrize("wavetype,param", [(1, 1), (2, 1), (1, 3), (3, 3)])
+def test_elastic_model_reader_matches_readmod_elastic(wavetype, param):
+    """The elastic reader (src/readmod_elastic.c): .vp / .vs / .rho, or under
+    PARAMETERIZATION 3 .lam / .mu / .rho, into the pi, u, rho slots."""
+    from ifos_b200 import workloads as W
+    ref, _ = H.libs()
+    rng = np.random.default_rng(23)
+    nx, ny = 11, 8
+    a = rng.uniform(1.0e9, 9.0e9, (ny, nx)).astype(np.float32)
+    b = rng.uniform(0.5e9, 3.0e9, (ny, nx)).astype(np.float32)
+    m = {("lam" if param == 3 else "vp"): a, ("mu" if param == 3 else "vs"): b,
+         "rho": rng.uniform(1800, 2600, (ny, nx)).astype(np.float32)}
+    if wavetype == 2:
+        del m["vp"]
+    prefix = os.path.join(tempfile.mkdtemp(prefix="md"), "m")
+    W.write_model(m, prefix)
+    H.set_globals(NX=nx, NY=ny, POS=[0, 0, 0], WAVETYPE=wavetype, PARAMETERIZATION=param, MYID=1)
+    for name, v in (("NXG", nx), ("NYG", ny), ("IDX", 1), ("IDY", 1)):
+        C.c_int.in_dll(ref, name).value = v
+    (C.c_char * 74).in_dll(ref, "MFILE").value = prefix.encode()
+    libc = _libc()
+    log = libc.fopen(os.devnull.encode(), b"w")
+    C.c_void_p.in_dll(ref, "FP").value = log
+    mats = [ref.matrix(1, ny, 1, nx) for _ in range(3)]  # rho, pi, u
+    f = ref.readmod_elastic
+    f.restype = None
+    f.argtypes = [H.FPP] * 3
+    f(*mats)
+    libc.fclose(log)
+    want = {k: np.array([[mats[q][j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
+            for q, k in enumerate(("rho", "vp", "vs")) if wavetype != 2 or k != "vp"}
+    got = W.read_model(prefix, nx, ny, wavetype=wavetype, parameterization=param)
+    assert sorted(got) == sorted(want)
+    for k, v in want.items():
+        assert np.array_equal(got[k].view(np.int32), v.view(np.int32)), k
 
 
 def test_model_reader_rejects_files_of_the_wrong_size():
