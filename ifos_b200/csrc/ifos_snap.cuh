@@ -794,6 +794,17 @@ __global__ void k_taper_shot(float *gout, long long n, int nx, int ny, unsigned 
     (void)ny;
 }
 
+// Per-shot gradient taper read from a file (src/taper_grad_shot.c:206-289,
+// sws 2-4): the planes of `planes` of one slot's stored gradients times the
+// coefficient plane, one float product per cell as waveconv *= taper_coeff.
+__global__ void k_taper_coeff(float *g, long long n, unsigned planes, const float *coeff) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const float t = coeff[q];
+    for (int k = 0; k < 10; k++)
+        if (planes >> k & 1u) g[k * n + q] *= t;
+}
+
 // Median smoothing of a gradient or model plane (src/smooth.c with
 // src/median2D.c).  Every cell takes the window of fs x fs values around it
 // (edges extended by the nearest row / column), gathered x-major as the

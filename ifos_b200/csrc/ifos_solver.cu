@@ -1618,6 +1618,22 @@ extern "C" int ifos_taper_grad_shot(ifos_ctx *c, int nshots, const float *src_xy
     return IFOS_OK;
 }
 
+extern "C" int ifos_taper_grad_coeff(ifos_ctx *c, int slot, unsigned planes, const float *coeff) {
+    if (!c || !coeff || slot < 0 || slot >= c->p.max_shots) return IFOS_ERR_ARG;
+    if (planes >> IFOS_NG) return fail(c, IFOS_ERR_ARG, "planes is a mask over the IFOS_NG gradient planes");
+    CK(cudaSetDevice(c->device));
+    if (int rc = order_after_fetches(c, false, true)) return rc;
+    const long long N = (long long)c->p.nx * c->p.ny;
+    void *scr = nullptr;
+    if (int rc = scratch(c, (size_t)N * 4, &scr)) return rc;
+    CK(cudaMemcpyAsync(scr, coeff, (size_t)N * 4, cudaMemcpyHostToDevice, c->st));
+    k_taper_coeff<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>((float *)c->gout.p + (long long)slot * IFOS_NG * N,
+                                                                  N, planes, (const float *)scr);
+    c->launches++;
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
 extern "C" int ifos_mat_change_test(ifos_ctx *c, const ifos_mat_change *mc, float *vp, float *vs, float *rho,
                                     const float *g_vp, const float *g_vs, const float *g_rho, const float *vp_start,
                                     const float *vs_start, const float *rho_start, float *vp1, float *vs1,

@@ -77,3 +77,39 @@ def write_matrix_disk(plane, name: str) -> str:
     path = f"{name}.bin"
     _write(path, _values(plane), BINARY)
     return path
+
+
+TAPER_KINDS = {2: "vp", 3: "vs", 4: "rho"}
+
+
+def taper_file_path(taper_file_name: str, ishot: int, sws: int, workflow_stage=None) -> str:
+    """The per-shot taper file src/taper_grad_shot.c:213-262 opens for sws 2
+    (vp), 3 (vs) and 4 (rho): ``<TAPER_FILE_NAME>.shot<ishot>.<kind>``; with
+    USE_WORKFLOW first ``...shot<ishot>_<WORKFLOW_STAGE>.<kind>``, then the
+    plain name."""
+    import os
+    kind = TAPER_KINDS[sws]
+    if workflow_stage is not None:
+        path = f"{taper_file_name}.shot{ishot}_{int(workflow_stage)}.{kind}"
+        if os.path.exists(path):
+            return path
+    path = f"{taper_file_name}.shot{ishot}.{kind}"
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"Taper file could not be opened: {path}")
+    return path
+
+
+def read_taper_file(taper_file_name: str, ishot: int, sws: int, nx: int, ny: int, workflow_stage=None) -> np.ndarray:
+    """The NY x NX coefficient plane of a per-shot taper file, read as
+    src/taper_grad_shot.c:268-281 reads it: NX*NY raw floats, x outer, y
+    inner.  The reference does not check the size: values past NX*NY are
+    ignored, and where the file ends early each remaining cell keeps the
+    last value read (its fread leaves grad_tap unchanged); an empty file,
+    which leaves grad_tap unset there, raises ValueError here."""
+    path = taper_file_path(taper_file_name, ishot, sws, workflow_stage)
+    vals = np.fromfile(path, np.float32, count=nx * ny)
+    if vals.size == 0:
+        raise ValueError(f"taper file {path} holds no values")
+    if vals.size < nx * ny:
+        vals = np.concatenate([vals, np.full(nx * ny - vals.size, vals[-1], np.float32)])
+    return np.ascontiguousarray(vals.reshape(nx, ny).T)

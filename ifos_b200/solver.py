@@ -319,6 +319,19 @@ class ShotSolver:
         self._check(self.lib.ifos_taper_grad_shot(self._ctx, int(nshots), _fp(xy), float(srtradius), int(srtshape),
                                                   int(filtsize), mask))
 
+    def taper_grad_coeff(self, slot, coeff, planes=(3,)):
+        """Multiply the stored gradients of `slot` (IFOS_G_* indices in
+        `planes`) by the NY x NX taper plane `coeff`, as
+        src/taper_grad_shot.c does with a taper file (sws 2-4; read the file
+        with ``modelio.read_taper_file``)."""
+        c = _f32(coeff)
+        if c.shape != (self.p.ny, self.p.nx):
+            raise ValueError(f"taper plane must be NY x NX = {(self.p.ny, self.p.nx)}, got {c.shape}")
+        mask = 0
+        for k in planes:
+            mask |= 1 << int(k)
+        self._check(self.lib.ifos_taper_grad_coeff(self._ctx, int(slot), mask, _fp(c)))
+
     def median_smooth(self, plane, filt_size):
         """Median smoothing of an NY x NX plane (src/smooth.c); returns a
         new array."""

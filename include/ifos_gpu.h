@@ -330,6 +330,16 @@ int ifos_timedomain_filt(ifos_ctx *ctx, float *data, int ntr, int ns, float fc, 
 int ifos_taper_grad_shot(ifos_ctx *ctx, int nshots, const float *src_xy, float srtradius, int srtshape,
                          int filtsize, unsigned planes);
 
+/* Per-shot gradient taper read from a file (src/taper_grad_shot.c:206-289,
+ * sws 2-4; the driver's SWS_TAPER_FILE_PER_SHOT, src/IFOS2D.c:2669-2697):
+ * the planes of `planes` (a bit mask over IFOS_G_*) of slot `slot`'s stored
+ * gradients are multiplied cell by cell by `coeff`, an NY x NX host plane --
+ * the TAPER_FILE_NAME.shot<n>.vp / .vs / .rho values, which the reference
+ * reads x-major (ifos_b200.modelio.read_taper_file reads them so).  The
+ * driver applies .vp to IFOS_G_VP, .vs to IFOS_G_VS and IFOS_G_VS_Z, .rho to
+ * IFOS_G_RHO and IFOS_G_RHO_Z. */
+int ifos_taper_grad_coeff(ifos_ctx *ctx, int slot, unsigned planes, const float *coeff);
+
 /* Median smoothing of an NY x NX plane (host, in place) as src/smooth.c
  * does for gradients (FILT_SIZE_GRAD) and models (FILT_SIZE): filt_size 0
  * leaves the plane unchanged, an even size grows away from zero, |size| up

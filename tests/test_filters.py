@@ -91,6 +91,63 @@ def test_shot_taper_matches_taper_grad_shot(srtradius, srtshape, filtsize, sx):
     assert np.array_equal(after[[0, 1, 2, 6, 7]], before[[0, 1, 2, 6, 7]])  # planes not asked for are untouched
 
 
+def test_taper_files_match_taper_grad_shot():
+    """The per-shot taper files (sws 2-4, the driver's SWS_TAPER_FILE_PER_SHOT,
+    src/IFOS2D.c:2669-2697) on two slots' stored gradients against
+    src/taper_grad_shot.c applied to the same planes with the same files:
+    .vp on the vp gradient, .vs on vs and SH vs, .rho on rho and SH rho."""
+    import tempfile
+    from ifos_b200 import modelio
+    from ifos_b200.solver import ShotSolver
+    from tests.golden.cases import build_case
+    ref, _ = H.libs()
+    p, model, g, sig, adj = build_case("psv_el_o4")
+    p.wavetype = 3
+    d = tempfile.mkdtemp(prefix="tp", dir="/tmp")
+    base = os.path.join(d, "taper")
+    rng = np.random.default_rng(9)
+    for ishot in (1, 2):
+        for kind in ("vp", "vs", "rho"):
+            rng.uniform(0.0, 1.0, p.nx * p.ny).astype(np.float32).tofile(f"{base}.shot{ishot}.{kind}")
+    planes = {2: (3,), 3: (4, 8), 4: (5, 9)}
+    with ShotSolver(p, max_shots=2, max_rec=g.recpos.shape[1]) as s:
+        s.upload_model(model)
+        for k in range(2):
+            s.setup_shot(k, g.srcpos, sig, g.recpos)
+        s.forward(2, store=True, fetch=False)
+        before = s.adjoint(np.stack([adj, adj * 0.5]), 2)
+        for k in range(2):
+            for sws, pl in planes.items():
+                s.taper_grad_coeff(k, modelio.read_taper_file(base, k + 1, sws, p.nx, p.ny), planes=pl)
+        after = s.fetch_grads(2)
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    C.c_void_p.in_dll(ref, "FP").value = libc.fopen(os.devnull.encode(), b"w")
+    for name, v in (("NX", p.nx), ("NY", p.ny), ("NXG", p.nx), ("NYG", p.ny), ("NPROCX", 1), ("NPROCY", 1),
+                    ("MYID", 0), ("VERBOSE", 0), ("USE_WORKFLOW", 0)):
+        C.c_int.in_dll(ref, name).value = v
+    pos = (C.c_int * 3).in_dll(ref, "POS")
+    pos[0] = pos[1] = pos[2] = 0
+    (C.c_char * 74).in_dll(ref, "TAPER_FILE_NAME").value = base.encode()
+    f = ref.taper_grad_shot
+    f.restype = None
+    f.argtypes = [H.FPP, H.FPP, H.FPP, C.c_int, H.IPP, C.c_int, C.c_int, C.c_int]
+    T = ref.matrix(1, p.ny, 1, p.nx)
+    for k in range(2):
+        for sws, pl in planes.items():
+            for plane in pl:
+                W_ = ref.matrix(1, p.ny, 1, p.nx)
+                for j in range(p.ny):
+                    for i in range(p.nx):
+                        W_[j + 1][i + 1] = float(before[k, plane, j, i])
+                f(W_, T, None, 0, None, 0, k + 1, sws)
+                want = np.array([[W_[j + 1][i + 1] for i in range(p.nx)] for j in range(p.ny)], np.float32)
+                assert np.array_equal(after[k, plane].view(np.int32), want.view(np.int32)), (k, plane)
+                assert not np.array_equal(after[k, plane], before[k, plane])
+    assert np.array_equal(after[:, [0, 1, 2, 6, 7]], before[:, [0, 1, 2, 6, 7]])
+
+
 @pytest.mark.parametrize("filt_size", [3, 4, 7, -5])
 def test_median_smoothing_matches_smooth(filt_size):
     """Median smoothing of a plane against src/smooth.c (filter 2, FILT_SIZE)

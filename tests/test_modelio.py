@@ -88,3 +88,49 @@ def test_mergemod_joins_rank_files_in_the_reference_order():
     got = np.fromfile(name, np.float32)
     want = np.concatenate([blocks[(ip, jp)].T[i] for ip in range(2) for i in range(3) for jp in range(2)])
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("sws,stage,trim", [(2, None, 0), (3, None, 0), (4, None, 5), (3, 2, 0), (4, 7, 0)])
+def test_taper_file_reader_matches_taper_grad_shot(sws, stage, trim):
+    """The per-shot taper files of src/taper_grad_shot.c (sws 2, 3, 4 ->
+    .vp, .vs, .rho) read as the reference reads them: x outer, the workflow
+    file (stage 2 here) before the plain one, the plain one when the workflow
+    file is missing (stage 7), and a file short by `trim` values whose last
+    cells keep the last value read.  The reference multiplies a plane of
+    ones by what it read, so the plane it returns is its coefficient plane."""
+    from tests import compat_harness as H
+    ref, _ = H.libs()
+    nx, ny, ishot = 11, 8, 3
+    rng = np.random.default_rng(sws + (stage or 0))
+    kind = modelio.TAPER_KINDS[sws]
+    d = tempfile.mkdtemp(prefix="tp", dir="/tmp")  # TAPER_FILE_NAME holds 74 characters
+    base = os.path.join(d, "taper")
+    rng.uniform(0.0, 1.0, nx * ny - trim).astype(np.float32).tofile(f"{base}.shot{ishot}.{kind}")
+    if stage == 2:
+        rng.uniform(2.0, 3.0, nx * ny).astype(np.float32).tofile(f"{base}.shot{ishot}_{stage}.{kind}")
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    C.c_void_p.in_dll(ref, "FP").value = libc.fopen(os.devnull.encode(), b"w")
+    for name, v in (("NX", nx), ("NY", ny), ("NXG", nx), ("NYG", ny), ("NPROCX", 1), ("NPROCY", 1), ("MYID", 0),
+                    ("VERBOSE", 0), ("USE_WORKFLOW", int(stage is not None)), ("WORKFLOW_STAGE", stage or 0)):
+        C.c_int.in_dll(ref, name).value = v
+    pos = (C.c_int * 3).in_dll(ref, "POS")
+    pos[0] = pos[1] = pos[2] = 0
+    (C.c_char * 74).in_dll(ref, "TAPER_FILE_NAME").value = base.encode()
+    W = ref.matrix(1, ny, 1, nx)
+    for j in range(ny):
+        for i in range(nx):
+            W[j + 1][i + 1] = 1.0
+    T = ref.matrix(1, ny, 1, nx)
+    f = ref.taper_grad_shot
+    f.restype = None
+    f.argtypes = [H.FPP, H.FPP, H.FPP, C.c_int, H.IPP, C.c_int, C.c_int, C.c_int]
+    f(W, T, None, 0, None, 0, ishot, sws)
+    want = np.array([[W[j + 1][i + 1] for i in range(nx)] for j in range(ny)], np.float32)
+    got = modelio.read_taper_file(base, ishot, sws, nx, ny, workflow_stage=stage)
+    assert np.array_equal(got.view(np.int32), want.view(np.int32))
+    if stage == 2:
+        assert got.min() >= 2.0  # the workflow file was read
+    with pytest.raises(FileNotFoundError):
+        modelio.read_taper_file(base, ishot + 1, sws, nx, ny)
