@@ -69,11 +69,13 @@ def _run(pair, fname, args, check_source_type=False):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fdorder,free_surf,sw,rng_kind", [
-    (2, 1, 0, "full"), (4, 0, 0, "full"), (6, 1, 1, "part"), (8, 1, 1, "full"), (10, 1, 0, "full"),
-    (12, 0, 1, "full"), (4, 1, 0, "part")])
-def test_update_v_PML(fdorder, free_surf, sw, rng_kind):
-    g = _base(fdorder, free_surf, ADJOINT_TYPE=1 + fdorder % 3)
+@pytest.mark.parametrize("fdorder,free_surf,sw,rng_kind,velocity", [
+    (2, 1, 0, "full", 0), (4, 0, 0, "full", 0), (6, 1, 1, "part", 0), (8, 1, 1, "full", 0), (10, 1, 0, "full", 0),
+    (12, 0, 1, "full", 0), (4, 1, 0, "part", 0),
+    # VELOCITY=1 (velocity seismograms inverted): vxp1 = vx in the adjoint (src/update_v_PML.c:143-151)
+    (4, 1, 1, "full", 1), (8, 0, 0, "part", 1)])
+def test_update_v_PML(fdorder, free_surf, sw, rng_kind, velocity):
+    g = _base(fdorder, free_surf, ADJOINT_TYPE=1 + fdorder % 3, VELOCITY=velocity)
     pair = H.Pair(g, 10 + fdorder)
     for n in ("vx", "vy", "vxp1", "vyp1", "vxm1", "vym1", "uttx", "utty", "sxx", "syy", "sxy", "absorb"):
         pair.field(n)
@@ -331,9 +333,9 @@ def test_update_s_visc_PML_SH(fdorder, free_surf, L):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fdorder,free_surf,sw", [(4, 1, 0), (8, 0, 1), (12, 1, 0)])
-def test_update_v_acoustic_PML(fdorder, free_surf, sw):
-    g = _base(fdorder, free_surf, ACOUSTIC=1, ADJOINT_TYPE=3)
+@pytest.mark.parametrize("fdorder,free_surf,sw,velocity", [(4, 1, 0, 0), (8, 0, 1, 0), (12, 1, 0, 0), (4, 0, 1, 1)])
+def test_update_v_acoustic_PML(fdorder, free_surf, sw, velocity):
+    g = _base(fdorder, free_surf, ACOUSTIC=1, ADJOINT_TYPE=3, VELOCITY=velocity)
     pair = H.Pair(g, 110 + fdorder)
     for n in ("vx", "vy", "vxp1", "vyp1", "vxm1", "vym1", "sp", "absorb"):
         pair.field(n)
