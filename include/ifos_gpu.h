@@ -398,11 +398,11 @@ int ifos_opt_step(const float *l2t, const float *epst, int fp64, float *opteps);
  * in *out (host).  Needs no context.  Its scratch is a static array of
  * IFOS_NOALLOC_MAX_BLOCKS+1 doubles that every device loading the library
  * keeps until exit; n is limited to IFOS_NOALLOC_MAX_N (IFOS_ERR_ARG above
- * it, message in ifos_last_error(NULL)).  The first call on a device resolves
- * the scratch address and should come before any stream capture.  Launches
- * go to `stream` (NULL: the default stream); the call copies the result to
- * host memory and waits for `stream` before it returns, so it must not be
- * called from a host function enqueued on a stream.  The calling thread's
+ * it, message in ifos_last_error(NULL)).  Launches go to `stream` (NULL:
+ * the default stream); the call copies the result to host memory and
+ * synchronises `stream` before it returns, so it can be called neither from
+ * a host function enqueued on a stream nor while any stream capture is in
+ * progress.  The calling thread's
  * current device is restored before returning.  All calls on a device share
  * the scratch, so calls that overlap on the GPU (other host threads, other
  * streams) race. */
