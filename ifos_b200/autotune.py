@@ -10,7 +10,9 @@ never what they compute (every setting is bit-identical):
   neighbouring CTAs the same tile of consecutive shots (shots per CTA
   neighbourhood), so that shots over one model read its coefficient tiles
   from L2.  Which wins depends on whether the model fits L2 and on the halo
-  reuse between vertically adjacent tiles.
+  reuse between vertically adjacent tiles.  2 and 3 are 0 and 1 with the
+  tiles that meet a CPML strip ranked first, which evens out the slower
+  strip tiles over the persistent CTAs.
 * ``pdl``: programmatic dependent launches between the loop's kernels.
 * ``graphs``: CUDA-graph replay of the time loops.
 * the batch size: shots stepped together per context, bounded by the
@@ -83,7 +85,7 @@ def short_params(p: ShotParams, snapshots: int = 6) -> ShotParams:
 
 
 def candidates(nshots: int, max_blocks: int = 3) -> List[dict]:
-    orders = (0, 1) if nshots > 1 else (0,)
+    orders = (0, 1, 2, 3) if nshots > 1 else (0, 2)
     out = []
     for bps, order, pdl in itertools.product([0] + list(range(1, max_blocks)), orders, (1, 0)):
         out.append(dict(graphs=1, pdl=pdl, blocks_per_sm=bps, tile_order=order))

@@ -363,6 +363,7 @@ extern "C" int ifos_ctx_create(const ifos_params *pp, int device, int with_snaps
     g.quirk_hi = (p.fdorder >= 10 && !p.hi_order_corrected && (c->psv || c->ac)) ? 1 : 0;
     g.mu_fix = p.mu_corrected ? 1 : 0;
     g.lame = p.parameterization == 3 ? 1 : 0;
+    g.tile_order = 2;  // CPML strip tiles first, slot-major (IFOS_OPT_TILE_ORDER)
     g.nt_total = p.nt;
     g.dt = p.dt;
     g.dh = p.dh;
@@ -1866,7 +1867,7 @@ extern "C" int ifos_set_option(ifos_ctx *c, int option, int value) {
             c->blocks_per_sm = value;
             break;
         case IFOS_OPT_TILE_ORDER:
-            if (value != 0 && value != 1) return fail(c, IFOS_ERR_ARG, "tile order must be 0 or 1");
+            if (value < 0 || value > 3) return fail(c, IFOS_ERR_ARG, "tile order must be 0..3");
             c->g.tile_order = value;
             break;
         case IFOS_OPT_WAIT_LIMIT:

@@ -131,9 +131,45 @@ struct __align__(16) TileInfo {
 // slot 1, ...; slot-minor order gives consecutive t the same tile of
 // consecutive slots, so the CTAs resident at one time share the model tiles
 // of shots over the same model (one HBM read, the rest from L2).
-__device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, int nshots, int slot_minor, TileInfo &r) {
+//
+// CPML-first order (tile order bit 1): the spatial rank runs over the tiles
+// that meet a CPML strip first -- the tile rows in a y strip (top without a
+// free surface, bottom), then the x-strip columns (left, right) of the other
+// rows -- and the interior last, each region row by row.  Strip tiles take
+// the slower CPML path of every op; ranked first, the round-robin of tiles
+// over the persistent CTAs hands each CTA the same number of them (within
+// one), so the CTAs finish together instead of the ones that drew the strip
+// columns finishing last.  A bijection on [0, ntx*nty).
+__device__ __forceinline__ int cpml_first(int rank, int ntx, int nty, int TY, const KGrid &g) {
+    if (g.fw <= 0) return rank;
+    const int cl = min(ntx, (g.fw - 1) / kTileX + 1);  // tile columns with i0 <= FW
+    const int vx = g.nx - g.fw + 1 - kTileX;            // right strip: min(i0+63, NX) >= NX-FW+1
+    const int xr0 = max(cl, vx <= 0 ? 0 : (vx + kTileX - 1) / kTileX);
+    const int rt = g.free_surf ? 0 : min(nty, (g.fw - 1) / TY + 1);  // tile rows with j0 <= FW
+    const int vy = g.ny - g.fw + 1 - TY;                              // bottom strip: j0+TY-1 >= NY-FW+1
+    const int yb0 = min(nty, max(rt, vy <= 0 ? 0 : (vy + TY - 1) / TY));
+    const int nys = rt + (nty - yb0);  // rows in a y strip
+    if (rank < nys * ntx) {
+        const int r = rank / ntx;
+        return (r < rt ? r : yb0 + (r - rt)) * ntx + (rank - r * ntx);
+    }
+    rank -= nys * ntx;
+    const int ce = cl + (ntx - xr0);  // x-strip columns
+    const int mid = nty - nys;        // rows between the y strips: rt .. yb0-1
+    if (rank < mid * ce) {
+        const int r = rank / ce, c = rank - r * ce;
+        return (rt + r) * ntx + (c < cl ? c : xr0 + (c - cl));
+    }
+    rank -= mid * ce;
+    const int w = ntx - ce;  // > 0 here: the regions above hold every tile when it is 0
+    const int r = rank / w;
+    return (rt + r) * ntx + cl + (rank - r * w);
+}
+
+__device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, int nshots, int order, const KGrid &g,
+                                        TileInfo &r) {
     int rem;
-    if (slot_minor) {
+    if (order & 1) {
         rem = t / nshots;
         r.slot = t - rem * nshots;
     } else {
@@ -141,6 +177,7 @@ __device__ __forceinline__ void tile_of(int t, int ntx, int nty, int TY, int nsh
         r.slot = t / per;
         rem = t - r.slot * per;
     }
+    if (order & 2) rem = cpml_first(rem, ntx, nty, TY, g);
     const int tyi = rem / ntx;
     r.i0 = (rem - tyi * ntx) * kTileX + 1;
     r.j0 = tyi * TY + 1;
@@ -200,7 +237,7 @@ __device__ __forceinline__ void run_pipeline(const KGrid &g, const KMaps &mp, in
         auto issue = [&](int k, bool halo, bool plain) {
             const int st = k % NST;
             TileInfo ti;
-            tile_of(blockIdx.x + k * gridDim.x, ntx, nty, TY, nshots, g.tile_order, ti);
+            tile_of(blockIdx.x + k * gridDim.x, ntx, nty, TY, nshots, g.tile_order, g, ti);
             float *stage = smem + st * P::STAGE;
             uint64_t *bar = &full[st];
             if (plain) {

@@ -115,15 +115,16 @@ class GpuBackend:
                snap_format: str, model: Optional[dict] = None):
         """A context for the batch.  Its execution options are the ones the
         autotuner picked on the measured workloads (graph replay, no PDL,
-        slot-minor tiles for several shots); with ``tune`` they are timed
+        slot-minor tiles for several shots, CPML strip tiles first for one);
+        with ``tune`` they are timed
         once per shape (at two shots, then cached) instead."""
         from .solver import ShotSolver
-        opts = dict(graphs=1, pdl=0, tile_order=1 if nshots > 1 else 0)
+        opts = dict(graphs=1, pdl=0, tile_order=1 if nshots > 1 else 2)
         if self.tune and model is not None and kind == GRADIENT:
             from . import autotune
             opts = autotune.tune(p, model, 2, snap_format, self.device)
             if nshots == 1:
-                opts["tile_order"] = 0
+                opts["tile_order"] = 2
         s = ShotSolver(p, max_shots=nshots, max_models=max_models, max_src=max_src, max_rec=max_rec,
                        snapshots=(kind == GRADIENT), snap_format=snap_format, device=self.device)
         if opts:

@@ -12,8 +12,8 @@ from ifos_b200.params import ShotParams
 def test_candidates_cover_the_knobs():
     one = A.candidates(1)
     many = A.candidates(4)
-    assert {c["tile_order"] for c in one} == {0}
-    assert {c["tile_order"] for c in many} == {0, 1}
+    assert {c["tile_order"] for c in one} == {0, 2}
+    assert {c["tile_order"] for c in many} == {0, 1, 2, 3}
     assert {c["blocks_per_sm"] for c in many} == {0, 1, 2}
     assert {c["pdl"] for c in many} == {0, 1}
     assert len(many) == 2 * len(one)
@@ -40,9 +40,9 @@ def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
     best = A.tune(p, {}, nshots=4)
     assert best == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=0)
     again = A.tune(p, {}, nshots=4)
-    assert again == best and calls == [12]  # second call served from the cache
+    assert again == best and calls == [24]  # second call served from the cache
     data = json.load(open(tmp_path / "tune.json"))
-    assert len(data) == 1 and len(next(iter(data.values()))["timed"]) == 12
+    assert len(data) == 1 and len(next(iter(data.values()))["timed"]) == 24
 
 
 @pytest.mark.gpu

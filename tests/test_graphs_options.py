@@ -59,7 +59,7 @@ def test_options_keep_results_bit_identical():
     shots = _shots(p, g, 3, 11)
     ref = _run(p, model, shots, 3, graphs=0, pdl=1)[0]
     for opts in (dict(tile_order=1), dict(blocks_per_sm=1), dict(pdl=0), dict(graphs=1, tile_order=1, pdl=0),
-                 dict(blocks_per_sm=2, tile_order=1)):
+                 dict(blocks_per_sm=2, tile_order=1), dict(tile_order=2), dict(graphs=1, tile_order=3, pdl=0)):
         got = _run(p, model, shots, 3, **opts)[0]
         assert bit_equal(ref[0], got[0]), opts
         assert bit_equal(ref[1], got[1]), opts
@@ -68,10 +68,10 @@ def test_options_keep_results_bit_identical():
 def test_option_values_checked_and_reported():
     p, *_ = build_case("psv_el_o4")
     with ShotSolver(p, snapshots=False) as s:
-        assert s.options() == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=0, wait_limit=0)
+        assert s.options() == dict(graphs=1, pdl=1, blocks_per_sm=0, tile_order=2, wait_limit=0)
         s.set_options(tile_order=1, blocks_per_sm=2, graphs=0)
         assert s.options() == dict(graphs=0, pdl=1, blocks_per_sm=2, tile_order=1, wait_limit=0)
         with pytest.raises(Exception):
-            s.set_options(tile_order=2)
+            s.set_options(tile_order=4)
         with pytest.raises(Exception):
             s.set_options(blocks_per_sm=-1)
