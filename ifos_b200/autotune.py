@@ -149,9 +149,13 @@ def best_batch(p: ShotParams, model: dict, free_bytes: int, max_batch: int = 64,
                device: int = 0, sizes: Optional[Iterable[int]] = None) -> dict:
     """The batch size (shots per context) with the most shots per second
     among those whose context fits `free_bytes` at the full NT, each with its
-    tuned options.  Returns {"nshots", "options", "shots_per_s"}."""
+    tuned options.  Returns {"nshots", "options", "shots_per_s"}.  The sizes
+    tried are the powers of two and three times them (1, 2, 3, 4, 6, 8, 12,
+    ...) up to `max_batch`: on a large grid the snapshot memory, not a power
+    of two, bounds the batch (six 2000 x 600 NT 6000 shots fit where eight do
+    not)."""
     from .solver import ShotSolver
-    sizes = sorted(set(sizes or [1 << k for k in range(0, 12) if (1 << k) <= max_batch]))
+    sizes = sorted(set(sizes or [m << k for k in range(0, 12) for m in (1, 3) if (m << k) <= max_batch]))
     best = None
     for n in sizes:
         need = ShotSolver.bytes_needed(p, snapshots=True, max_shots=n, snap_format=snap_format)

@@ -64,3 +64,25 @@ def test_tuned_options_run_and_match(tmp_path, monkeypatch):
             sec = s.forward(1)
             res.append((sec, s.adjoint(adj[None])))
     assert bit_equal(res[0][0], res[1][0]) and bit_equal(res[0][1], res[1][1])
+
+
+def test_best_batch_tries_three_times_powers_of_two(monkeypatch):
+    """best_batch walks 1, 2, 3, 4, 6, 8, ... until a context no longer fits,
+    and takes a larger batch only when it is 3 % faster per shot (memory and
+    timing faked: 25 GB per shot, 151 GB free, per-shot cost falling with the
+    batch)."""
+    from ifos_b200.solver import ShotSolver
+    tried = []
+    monkeypatch.setattr(ShotSolver, "bytes_needed", staticmethod(lambda p, snapshots, max_shots, snap_format:
+                                                                  int(25e9) * max_shots))
+    monkeypatch.setattr(A, "tune", lambda p, model, n, fmt, dev: dict(graphs=1, tile_order=1))
+
+    def fake_time(p, model, n, options, snap_format="fp32", device=0, reps=3):
+        tried.append(n)
+        return [(n * (1.0 + 0.5 / n), options[0])]
+
+    monkeypatch.setattr(A, "time_options", fake_time)
+    p = ShotParams(nx=64, ny=40, nt=90, dtinv=3)
+    best = A.best_batch(p, {}, free_bytes=int(151e9), max_batch=8)
+    assert tried == [1, 2, 3, 4, 6]  # 8 shots need 200 GB
+    assert best["nshots"] == 6
