@@ -137,10 +137,13 @@ def test_single_steps_match():
         assert bit_equal(f[m], r[m]), n
 
 
-def test_batched_shots_and_models_match_single_runs():
+@pytest.mark.parametrize("tile_order", [2, 3])
+def test_batched_shots_and_models_match_single_runs(tile_order):
     """Three shots over two models in one context (one kernel per step for
     all of them) give exactly the single-shot results, and the gradient sum
-    matches the reference's shot-order accumulation."""
+    matches the reference's shot-order accumulation; with the tiles dealt
+    slot-major (2, the default) and slot-minor (3), CPML strip tiles first,
+    on a grid whose 60 columns fill less than one tile row."""
     p, true, start, geoms = W.plain_elastic(2, nt=80, nx=60, ny=40)
     p.fw = 8
     models = [true, start]
@@ -154,6 +157,7 @@ def test_batched_shots_and_models_match_single_runs():
         shots.append((k % 2, W.Geometry(src, rec), sig, adj))
     ntr = shots[0][1].recpos.shape[1]
     with ShotSolver(p, max_shots=3, max_models=2, max_rec=ntr) as s:
+        s.set_options(tile_order=tile_order)
         for i, m in enumerate(models):
             s.upload_model(m, i)
         for slot, (mi, g, sig, adj) in enumerate(shots):
