@@ -26,7 +26,7 @@ EXPORTS = [
     "ifos_kernel_times", "ifos_grad_sum_device", "ifos_set_stream", "ifos_dot_f64_noalloc", "ifos_last_ms", "ifos_launch_count",
     "ifos_sync", "ifos_trkill_table", "ifos_time_window", "ifos_set_option", "ifos_get_option",
     "ifos_residual_adjoint", "ifos_fetch_snapshot", "ifos_opt_step", "ifos_timedomain_filt",
-    "ifos_taper_grad_shot", "ifos_taper_grad_coeff", "ifos_median_smooth", "ifos_mat_change_test", "ifos_fetch_sections_async",
+    "ifos_taper_grad_shot", "ifos_taper_grad_coeff", "ifos_lbfgs_core", "ifos_median_smooth", "ifos_mat_change_test", "ifos_fetch_sections_async",
     "ifos_fetch_grads_async", "ifos_fetch_wait", "ifos_host_alloc", "ifos_host_free", "ifos_status",
 ]
 OPTIONS = {"graphs": 0, "pdl": 1, "blocks_per_sm": 2, "tile_order": 3, "wait_limit": 4}
@@ -128,6 +128,7 @@ def load():
         "ifos_timedomain_filt": (C.c_int, [vp, FP, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float]),
         "ifos_taper_grad_shot": (C.c_int, [vp, C.c_int, FP, C.c_float, C.c_int, C.c_int, C.c_uint]),
         "ifos_taper_grad_coeff": (C.c_int, [vp, C.c_int, C.c_uint, FP]),
+        "ifos_lbfgs_core": (C.c_int, [vp, C.c_int, C.c_int, C.c_size_t, FP, FP, FP, FP, FP, FP, C.c_int]),
         "ifos_median_smooth": (C.c_int, [vp, FP, C.c_int]),
         "ifos_fetch_sections_async": (C.c_int, [vp, C.c_int, FP]),
         "ifos_fetch_grads_async": (C.c_int, [vp, C.c_int, FP]),

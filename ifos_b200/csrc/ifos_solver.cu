@@ -1278,6 +1278,113 @@ extern "C" int ifos_dot_f64(ifos_ctx *c, const float *a, const float *b, size_t 
     return IFOS_OK;
 }
 
+// Vector updates of the L-BFGS two-loop recursion (src/LBFGS.c:285-321), each
+// the reference's float operation: mode 0 x = x - a*y, mode 1 x = a*y,
+// mode 2 x = x + y*a (a: alpha, h0, or alpha - beta, rounded to float).
+__global__ void k_lbfgs_vec(float *x, const float *y, float a, long long n, int mode) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        if (mode == 0) x[k] = x[k] - a * y[k];
+        else if (mode == 1) x[k] = a * y[k];
+        else x[k] = x[k] + y[k] * a;
+    }
+}
+
+// sum(a*b) in double over n device floats, on the context's stream, to the host
+static int dot_dev(ifos_ctx *c, const float *a, const float *b, long long n, double *out) {
+    const int nb = 592;
+    k_dot_partial<<<nb, 256, 0, c->st>>>(a, b, n, (double *)c->dot_partial.p);
+    k_dot_final<<<1, 256, 0, c->st>>>((const double *)c->dot_partial.p, nb, (double *)c->dot_out.p);
+    c->launches += 2;
+    CK(cudaMemcpyAsync(out, c->dot_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return IFOS_OK;
+}
+
+extern "C" int ifos_lbfgs_core(ifos_ctx *c, int iteration, int n_lbfgs, size_t npar, const float *s, const float *y,
+                               float *rho, float *q, float *alpha, float *r, int device_ptrs) {
+    if (!c || !s || !y || !rho || !q || !alpha || !r || n_lbfgs < 1 || iteration < 2 || npar < 1)
+        return IFOS_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    const long long n = (long long)npar;
+    const size_t vb = npar * sizeof(float), mb = (size_t)n_lbfgs * vb;
+    DevBuf ts, ty, tq, tr;
+    struct Frees {  // the staging copies of host arrays, freed on every return
+        DevBuf *b[4];
+        ~Frees() {
+            for (DevBuf *x : b) dev_free(*x);
+        }
+    } frees{{&ts, &ty, &tq, &tr}};
+    const float *ds = s, *dy = y;
+    float *dq = q, *dr = r;
+    if (!device_ptrs) {
+        int rc = dev_alloc(c, ts, mb);
+        if (!rc) rc = dev_alloc(c, ty, mb);
+        if (!rc) rc = dev_alloc(c, tq, vb);
+        if (!rc) rc = dev_alloc(c, tr, vb);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ts.p, s, mb, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(ty.p, y, mb, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(tq.p, q, vb, cudaMemcpyHostToDevice, c->st));
+        ds = (const float *)ts.p;
+        dy = (const float *)ty.p;
+        dq = (float *)tq.p;
+        dr = (float *)tr.p;
+    }
+    auto row = [&](const float *m, int w) { return m + (size_t)(w - 1) * npar; };  // pair w = 1..n_lbfgs
+    const unsigned nb = 4 * (unsigned)c->num_sms;
+    int rc = IFOS_OK;
+    int m = iteration - n_lbfgs;
+    if (m < 1) m = 1;
+    // H0 and rho of the newest pair (src/LBFGS.c:240-256)
+    int w = (iteration - 1) % n_lbfgs;
+    if (w == 0) w = n_lbfgs;
+    double d1 = 0.0, d2 = 0.0;
+    if (!rc) rc = dot_dev(c, row(dy, w), row(ds, w), n, &d1);
+    if (!rc) rc = dot_dev(c, row(dy, w), row(dy, w), n, &d2);
+    const float buf1 = (float)d1, buf2 = (float)d2;
+    rho[w - 1] = 1 / buf1;
+    const float h0 = buf1 / buf2;
+    // loop 1, newest pair first (:271-290)
+    for (int v = iteration - 1; v >= m && !rc; v--) {
+        int wv = v % n_lbfgs;
+        if (wv == 0) wv = n_lbfgs;
+        double sq = 0.0;
+        rc = dot_dev(c, row(ds, wv), dq, n, &sq);
+        alpha[wv - 1] = (float)((double)rho[wv - 1] * sq);
+        if (!rc) {
+            k_lbfgs_vec<<<nb, 256, 0, c->st>>>(dq, row(dy, wv), alpha[wv - 1], n, 0);
+            c->launches++;
+        }
+    }
+    // r = H0 q (:295-297), then loop 2, oldest pair first (:302-321)
+    if (!rc) {
+        k_lbfgs_vec<<<nb, 256, 0, c->st>>>(dr, dq, h0, n, 1);
+        c->launches++;
+    }
+    for (int v = m; v <= iteration - 1 && !rc; v++) {
+        int wv = v % n_lbfgs;
+        if (wv == 0) wv = n_lbfgs;
+        double yr = 0.0;
+        rc = dot_dev(c, row(dy, wv), dr, n, &yr);
+        const float beta = (float)((double)rho[wv - 1] * yr);
+        if (!rc) {
+            k_lbfgs_vec<<<nb, 256, 0, c->st>>>(dr, row(ds, wv), alpha[wv - 1] - beta, n, 2);
+            c->launches++;
+        }
+    }
+    if (!rc && !device_ptrs) {
+        cudaError_t e = cudaMemcpyAsync(q, dq, vb, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(r, dr, vb, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        if (e != cudaSuccess) rc = fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(c->st);
+        if (e != cudaSuccess) rc = fail(c, IFOS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return rc;
+}
+
 extern "C" int ifos_calc_res(ifos_ctx *c, int ntr, const float *obs, const float *syn, float *diff, double *l2,
                              double *energy) {
     if (!c || !obs || !syn || ntr < 1) return IFOS_ERR_ARG;

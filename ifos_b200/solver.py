@@ -332,6 +332,22 @@ class ShotSolver:
             mask |= 1 << int(k)
         self._check(self.lib.ifos_taper_grad_coeff(self._ctx, int(slot), mask, _fp(c)))
 
+    def lbfgs_core(self, iteration, s, y, rho, q):
+        """The L-BFGS two-loop recursion of src/LBFGS.c:226-323 with FP64 dot
+        products: s, y (n_lbfgs, npar) with row w-1 the pair w, rho
+        (n_lbfgs,), q (npar,) the gradient.  Returns (r, q, rho, alpha): the
+        direction, q as the recursion leaves it, rho with the newest pair's
+        entry set, and alpha."""
+        s, y = _f32(s), _f32(y)
+        n_lbfgs, npar = s.shape
+        rho = _f32(rho).copy()
+        q = _f32(q).copy()
+        alpha = np.zeros(n_lbfgs, np.float32)
+        r = np.zeros(npar, np.float32)
+        self._check(self.lib.ifos_lbfgs_core(self._ctx, int(iteration), int(n_lbfgs), int(npar), _fp(s), _fp(y),
+                                             _fp(rho), _fp(q), _fp(alpha), _fp(r), 0))
+        return r, q, rho, alpha
+
     def median_smooth(self, plane, filt_size):
         """Median smoothing of an NY x NX plane (src/smooth.c); returns a
         new array."""

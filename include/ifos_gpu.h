@@ -207,6 +207,21 @@ int ifos_fetch_fields(ifos_ctx *ctx, int slot, float *fields);
  * device: returns sum(a*b) (b NULL: sum(a*a)) accumulated in double. */
 int ifos_dot_f64(ifos_ctx *ctx, const float *a, const float *b, size_t n, int device_ptrs, double *out);
 
+/* The L-BFGS two-loop recursion (src/LBFGS.c:226-323, lbfgs_core, one rank)
+ * on the device.  s and y hold n_lbfgs rows of npar floats, row w-1 being
+ * the reference's s_LBFGS[w] / y_LBFGS[w] (w = 1..n_lbfgs, the ring the
+ * driver fills); q (npar) is the preconditioned gradient, changed in place as
+ * the reference changes it; r (npar) receives the direction; rho and alpha
+ * are host arrays of n_lbfgs floats: rho[w-1] of the newest pair
+ * (w = (iteration-1) % n_lbfgs, 0 read as n_lbfgs) is set, the others are
+ * read, and alpha is filled.  iteration >= 2.  device_ptrs: s, y, q and r are
+ * device pointers, else host arrays (copied in and out).  Every dot product
+ * is accumulated in double (the reference sums in float); its result is
+ * rounded to float where the reference keeps a float (rho, H0, alpha, beta),
+ * and the vector updates are the reference's float operations. */
+int ifos_lbfgs_core(ifos_ctx *ctx, int iteration, int n_lbfgs, size_t npar, const float *s, const float *y,
+                    float *rho, float *q, float *alpha, float *r, int device_ptrs);
+
 /* Residuals of one component, LNORM=2, VELOCITY=0 (src/calc_res.c:137-281):
  * integrates both sections, writes the time-reversed residual to diff
  * (ntr x NT) and the misfit/energy sums in double. */
