@@ -131,3 +131,30 @@ def test_device_lbfgs_core_matches_reference():
     assert abs(rho_out[w - 1] - rho64[w - 1]) <= abs(rho_ref[w - 1] - rho64[w - 1]) + 1e-6 * abs(rho64[w - 1])
     assert np.array_equal(np.delete(rho_out, w - 1), np.delete(rho, w - 1))  # the older pairs' rho untouched
     assert all(np.array_equal(a, b) for a, b in zip(again, (r, q_out, rho_out, alpha)))  # deterministic
+
+
+@pytest.mark.gpu
+def test_device_pointers_give_the_host_array_result():
+    """The same recursion on arrays already on the device (device_ptrs = 1,
+    torch tensors through the C ABI) equals the host-array call bit for
+    bit, and q is updated in place on the device."""
+    import torch
+    from ifos_b200.params import ShotParams
+    from ifos_b200.solver import ShotSolver
+    s, y, rho, q = _pairs(seed=5)
+    with ShotSolver(ShotParams(nx=32, ny=24, nt=20, dh=1.0, dt=1e-3, fdorder=4, fw=4), snapshots=False) as sol:
+        r_h, q_h, rho_h, a_h = sol.lbfgs_core(ITER, s, y, rho, q)
+        ds, dy, dq = (torch.from_numpy(a).cuda(0) for a in (s, y, q))
+        dr = torch.zeros(NPAR, dtype=torch.float32, device="cuda:0")
+        rho_d = rho.copy()
+        alpha_d = np.zeros(N_LBFGS, np.float32)
+        torch.cuda.synchronize()
+        fp = lambda a: C.cast(a.ctypes.data, C.POINTER(C.c_float))
+        dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_float))
+        rc = sol.lib.ifos_lbfgs_core(sol._ctx, ITER, N_LBFGS, NPAR, dp(ds), dp(dy), fp(rho_d), dp(dq), fp(alpha_d),
+                                     dp(dr), 1)
+        assert rc == 0
+        r_d, q_d = dr.cpu().numpy(), dq.cpu().numpy()
+    assert np.array_equal(r_d.view(np.int32), r_h.view(np.int32))
+    assert np.array_equal(q_d.view(np.int32), q_h.view(np.int32))
+    assert np.array_equal(rho_d, rho_h) and np.array_equal(alpha_d, a_h)
